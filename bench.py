@@ -1,0 +1,320 @@
+#!/usr/bin/env python
+"""Throughput of the cytokine-diffusion tick on B200.
+
+Workload (default): the human-scale world -- 8 fp32 fields on a 512x256x384
+grid (x fastest), Gaussian sigma = 1.5 x (1.2, 0.9, 1.0, 0.8, 1.1, 1.0, 1.3,
+0.9), decay (0.05, 0.01, 0.02, 0.03, 0.05, 0.04, 0.06, 0.02) per substep,
+200k lognormal(-6, 1) point sources per field, zero padding, seed 0.
+One step = one tick = 10 diffusion substeps of all 8 fields + source deposit
++ FP64 totals.  Metric: voxel-steps/s (data voxels x fields x substeps / s).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl vfd|reference]
+
+N > 1 runs under torchrun: every rank diffuses its own world (independent
+units, no data-path collective; weak scaling); the time is the max over
+ranks.  `--impl reference` times the CPU restatement of the path (the
+reference has no runnable CPU diffusion) on rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (os.path.join(ROOT, "vf-version_7_3_b200"), ROOT):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "voxel-steps/s"
+# ncu dram__bytes_read.sum + dram__bytes_write.sum per axis-pass launch of this
+# workload (8 fields), from profiles/axis_pass_cfg1.md; None until captured.
+AXIS_TRAFFIC_BYTES = None
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cfg_by_name(name):
+    from vfd import configs
+    return {"cfg0": configs.CFG0, "cfg1": configs.CFG1, "cfg4": configs.CFG4}[name]
+
+
+def workload_config(c, fft=None):
+    nx, ny, nz = c["grid"]
+    d = {"workload": f"{c['name']}: {nx}x{ny}x{nz} fp32 x 8 fields, {c['substeps']} substeps "
+                     f"per step (tick), {c['n_sources']} sources/field, zero padding, seed {c['seed']}",
+         "grid": [nx, ny, nz], "fields": 8, "substeps_per_step": c["substeps"],
+         "sources_per_field": c["n_sources"],
+         "l2": f"inputs larger than L2: {8 * nx * ny * nz * 4 / 1e9:.2f} GB of fields per world"}
+    if fft:
+        d["fft"] = list(fft)
+    return d
+
+
+def cpu_baseline(c, n_fields, nthreads=0):
+    """FP32 OpenMP CPU port (oracle/vfd_cpu_port.c): one substep of n_fields
+    fields of the workload plus their deposit; voxel-steps/s."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from vfd import configs
+    nx, ny, nz = c["grid"]
+    ins = configs.field_inputs(c["seed"], 0, c["grid"], c["n_sources"], n_fields=n_fields)
+    t0 = time.perf_counter()
+    for f, (u, idx, amt) in enumerate(ins):
+        s = c["sigma"][f]
+        oracle.port_substep(u, (s, s, s), (configs.radius(s),) * 3, c["decay"][f], nthreads=nthreads)
+        oracle.port_deposit_total(u, idx, amt)
+    dt = time.perf_counter() - t0
+    vs = nx * ny * nz * n_fields
+    return {"value": vs / dt, "unit": METRIC, "cores": oracle.port_threads() if nthreads <= 0 else nthreads,
+            "kind": "port",
+            "sample": f"{n_fields} field(s) x 1 substep + deposit of the {nx}x{ny}x{nz} world "
+                      f"({vs / 1e6:.1f} M voxel-steps), FP32 separable direct convolution, OpenMP",
+            "seconds": dt}
+
+
+def run_reference(args, c):
+    """--impl reference: the CPU restatement on the host cores (rank 0 only)."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    nf = 1
+    for _ in range(args.warmup):
+        cpu_baseline(c, nf)
+    vals = []
+    t_all = 0.0
+    for _ in range(args.steps):
+        r = cpu_baseline(c, nf)
+        vals.append(r["value"])
+        t_all += r["seconds"]
+    value = args.steps / sum(1.0 / v for v in vals)
+    cb = cpu_baseline.__doc__
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_all / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(c), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": r["cores"], "kind": "port",
+                             "sample": r["sample"] + "; each step is this sample"},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference's CPU diffusion (Diffuser::diffuseChemCPU) does not run; "
+                    "this arm times the FP32 OpenMP restatement of the same method"}
+    del cb
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="vfd", choices=["vfd", "reference"])
+    ap.add_argument("--config", default="cfg1", choices=["cfg0", "cfg1", "cfg4"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-fields", type=int, default=2,
+                    help="fields in the CPU-baseline sample (1 substep each)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    c = cfg_by_name(args.config)
+    if args.impl == "reference":
+        run_reference(args, c)
+        return
+
+    import numpy as np
+    import torch
+
+    import vfd
+    from vfd import configs
+
+    ws, rank, local = dist_env()
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = local
+    torch.cuda.set_device(dev)
+    nx, ny, nz = c["grid"]
+    V = nx * ny * nz
+    nf = 8
+    params = [vfd.field_params(s, d) for s, d in zip(c["sigma"], c["decay"])]
+    world = vfd.World(nx, ny, nz, params, device=dev)
+    ins = configs.field_inputs(c["seed"], rank, c["grid"], c["n_sources"])
+    for f, (u, idx, amt) in enumerate(ins):
+        world.upload(f, u)
+        world.set_sources(f, idx, amt)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        world.tick(c["substeps"], stream=sh)
+    torch.cuda.synchronize(dev)
+    world.set_profiling(True)
+    world.read_profile()
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    l0 = vfd.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        world.tick(c["substeps"], stream=sh)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    launches = vfd.launch_count() - l0
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    prof = world.read_profile()
+    world.set_profiling(False)
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    vsteps = V * nf * c["substeps"] * args.steps
+    value = ws * vsteps / (ms / 1e3)
+
+    # roofline of the dominant kernel (axis pass): 8 B per voxel per field per launch
+    axis_ms = sum(prof[k][0] for k in ("x", "y", "z"))
+    axis_n = sum(prof[k][1] for k in ("x", "y", "z"))
+    avg_ms = axis_ms / max(axis_n, 1)
+    alg_bytes = 8.0 * V * nf
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (avg_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": AXIS_TRAFFIC_BYTES,
+                "kernel": "axis_pass_kernel (x, y, z passes)",
+                "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
+                "peak_source": f"{peak_kind} hbm_gbs",
+                "share_of_step": axis_ms / ms if ms > 0 else None,
+                "per_pass_ms": {k: prof[k][0] / max(prof[k][1], 1) for k in prof}}
+
+    # e2e through the host-buffer entry point (H2D + tick + D2H every step)
+    pin_in = [torch.empty(V, dtype=torch.float32, pin_memory=True) for _ in range(nf)]
+    pin_out = [torch.empty(V, dtype=torch.float32, pin_memory=True) for _ in range(nf)]
+    host_in = [p.numpy() for p in pin_in]
+    host_out = [p.numpy() for p in pin_out]
+    for f in range(nf):
+        host_in[f][:] = ins[f][0].ravel()
+    world.diffuse_host(host_in, host_out, c["substeps"])
+    barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        for f, (u, idx, amt) in enumerate(ins):
+            world.set_sources(f, idx, amt)
+        world.diffuse_host(host_in, host_out, c["substeps"])
+    t_e2e = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([t_e2e], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = {"value": ws * V * nf * c["substeps"] * args.e2e_steps / t_e2e, "unit": METRIC,
+           "h2d_bytes_per_step": nf * V * 4 + sum(i.nbytes + a.nbytes for _, i, a in ins),
+           "d2h_bytes_per_step": nf * V * 4,
+           "api": "vfd_diffuse_host (pinned host buffers in and out, the diffuseChemGPU contract)",
+           "steps": args.e2e_steps}
+
+    line = None
+    if rank == 0:
+        cb = None
+        if not args.no_cpu_baseline and ws == 1:
+            cb = cpu_baseline(c, args.cpu_fields)
+            cb.pop("seconds", None)
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic (seeded counter-based generator)",
+                "config": workload_config(c, world.fft_dims()), "roofline": roofline,
+                "cpu_baseline": cb, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+    world.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

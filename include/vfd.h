@@ -1,0 +1,173 @@
+/*
+ * vfd.h -- C ABI of the B200 cytokine-diffusion library (libvfd.so).
+ *
+ * Replaces the diffusion layer of the vocal-fold ABM (src/Diffusion/ in the
+ * reference): the per-tick FFT-convolution diffusion of the chemical fields
+ * that WHWorld::diffuseCytokines() drives through
+ * Diffuser::diffuseChemGPU(int rightWallIndex)
+ * (src/World/Usr_World/woundHealingWorld.cpp:2403-2407,
+ *  src/Diffusion/Diffuser.cpp:221-470).
+ *
+ * Plain C types only: pointers, sizes, ints, doubles.  A CUDA stream is
+ * passed as void* (cudaStream_t); NULL means the legacy default stream.
+ * Every entry point returns a vfd_status; none exits, aborts or traps.
+ *
+ * Data layout (unchanged from the reference): one fp32 array of nx*ny*nz
+ * voxels per field, index = x + nx*(y + ny*z), x fastest
+ * (src/FieldVariable/Usr_FieldVariables/WHChemical.cpp:424).
+ *
+ * Threading: a world is bound to one device.  Calls on different worlds are
+ * thread-safe; calls on one world must be serialised by the caller (the
+ * reference calls its Diffuser from one OpenMP thread,
+ * woundHealingWorld.cpp:2013-2026).
+ */
+#ifndef VFD_H_
+#define VFD_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference has none: checkCudaErrors() exits the
+ * process and fftDiffuse3D's bool is ignored (Diffuser.cpp:139-148). */
+typedef enum vfd_status {
+    VFD_OK = 0,
+    VFD_ERR_INVALID_ARG = 1,
+    VFD_ERR_OUT_OF_MEMORY = 2,
+    VFD_ERR_BUDGET = 3,       /* admission refused by an HBM budget      */
+    VFD_ERR_CUDA = 4,         /* a CUDA runtime call failed              */
+    VFD_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up      */
+    VFD_ERR_DEVICE_FAULT = 6, /* a kernel reported a bad index/argument  */
+    VFD_ERR_NOT_SUPPORTED = 7,
+    VFD_ERR_NO_DEVICE = 8
+} vfd_status;
+
+/* Boundary treatment of the padded FFT grid.
+ * VFD_PAD_ZERO: the field is zero-extended (BASELINE configurations).
+ * VFD_PAD_CONSTANT_VF: the reference's padDataConstantVF3D rule
+ *   (src/Diffusion/convolutionFFT.cuh:590-638): only 0<z<nz-1, 0<y<ny-1,
+ *   0<x<epi_boundary keeps the field value; every other voxel of the FFT
+ *   grid (padding, outer data shell, x >= epi_boundary) holds `baseline`. */
+typedef enum vfd_pad_mode {
+    VFD_PAD_ZERO = 0,
+    VFD_PAD_CONSTANT_VF = 1
+} vfd_pad_mode;
+
+/* Per-field diffusion parameters.
+ * Kernel: normalised sampled Gaussian exp(-j^2/(2 sigma^2)) per axis,
+ * truncated to [-radius, radius] on each axis and normalised in FP64 (the
+ * product over the cube is therefore normalised too).  This is the
+ * heat-kernel counterpart of the reference's window (the explicit 7-point
+ * stencil raised to a power, src/Diffusion/Diffusion.cu:1078-1531).
+ * Substep: u <- (1 - decay_rate) * (baseline + conv(M .* (u - baseline))). */
+typedef struct vfd_field_params {
+    double sigma[3];    /* x, y, z, in voxels; > 0                       */
+    int radius[3];      /* <= 0 selects ceil(3 sigma)                    */
+    double decay_rate;  /* first-order decay per substep, in [0, 1)      */
+    float baseline;     /* reference pbaseline[ic] (woundHealingWorld.cpp:969);
+                           ignored by VFD_PAD_ZERO                        */
+} vfd_field_params;
+
+/* One world (one set of co-located fields on one grid).  The reference
+ * sizes this through c_ctx (src/Diffusion/convolutionFFT_common.h:305-346)
+ * and diffusion_helper::initChemDimensions (DiffusionHelper.cpp:381-461). */
+typedef struct vfd_world_desc {
+    int nx, ny, nz;
+    int n_fields;
+    const vfd_field_params *fields; /* n_fields entries                   */
+    int pad_mode;                   /* vfd_pad_mode                       */
+    int epi_boundary;               /* constant-VF x bound (rightWallIndex) */
+    int fft[3];                     /* FFT length per axis; 0 = planner   */
+} vfd_world_desc;
+
+typedef struct vfd_world vfd_world;
+
+/* Mass accounting per field, FP64 (WHChemical::update sums per-field totals
+ * in double, WHChemical.cpp:420-450).  Values refer to the last substep run
+ * (input_sum, leaked, conv_sum) and to the last tick (total, sources). */
+typedef struct vfd_mass {
+    double input_sum;   /* sum of M .* (u - b) entering the last substep  */
+    double leaked[3];   /* mass the kernel pushed past the crop, per axis */
+    double conv_sum;    /* sum of the cropped convolution (before +b, decay) */
+    double total;       /* sum of the field after the tick (incl. sources) */
+    double sources;     /* sum of the amounts deposited in the last tick  */
+    double reserved;
+} vfd_mass;
+
+/* ---- world lifetime (Diffuser ctor + diffusion_helper::alloc*Buffers,
+ *      Diffuser.cpp:27-35, DiffusionHelper.cpp:464-647) ------------------ */
+vfd_status vfd_world_create(const vfd_world_desc *desc, int device, vfd_world **out);
+vfd_status vfd_world_destroy(vfd_world *w);
+
+/* FFT grid the planner chose (Fx, Fy, Fz) -- the reference's FFTW/H/D. */
+vfd_status vfd_world_fft_dims(const vfd_world *w, int *fft3);
+/* Device bytes this world holds. */
+vfd_status vfd_world_device_bytes(const vfd_world *w, size_t *bytes);
+
+/* ---- field transfer (H2D / D2H, Diffusion.cu:72-122) ------------------ */
+vfd_status vfd_upload_field(vfd_world *w, int field, const float *host, void *stream);
+vfd_status vfd_download_field(vfd_world *w, int field, float *host, void *stream);
+/* Device pointer of a resident field (V floats, valid until destroy). */
+vfd_status vfd_field_device_ptr(vfd_world *w, int field, float **dptr);
+
+/* ---- sources (Agent::produce_* -> dChem[ic][voxel] += inc, Agent.cpp:185)
+ * Registers this field's point sources for every following tick: the
+ * arrays are copied to the device; idx are voxel indices in [0, V),
+ * duplicates accumulate.  n = 0 clears them. */
+vfd_status vfd_set_sources(vfd_world *w, int field, const int32_t *idx,
+                           const float *amt, int64_t n);
+
+/* ---- one tick: n_substeps diffusion substeps of every field, then the
+ * registered sources are deposited and the FP64 totals are formed.
+ * Replaces fftDiffuse3D (Diffusion.cu:1622-1934) for every chemical plus
+ * the deposit/total part of WHChemical::update (WHChemical.cpp:420-450).
+ * Fields stay on the device; asynchronous on `stream`. -------------------- */
+vfd_status vfd_tick(vfd_world *w, int n_substeps, void *stream);
+
+/* Mass accounting of each field (n_fields entries); synchronises `stream`. */
+vfd_status vfd_read_mass(vfd_world *w, vfd_mass *out, void *stream);
+
+/* ---- drop-in of Diffuser::diffuseChemGPU (Diffuser.cpp:221-470):
+ * for every field, host_in[f] -> device, one tick, device -> host_out[f]
+ * (the reference's h_ibuffs / h_obuffs, DiffusionHelper.cpp:529-531).
+ * Copies are pipelined against the compute of the other fields.  Host
+ * buffers may be pinned or pageable; host_out may equal host_in.
+ * Synchronous: returns when host_out holds the result. */
+vfd_status vfd_diffuse_host(vfd_world *w, const float *const *host_in,
+                            float *const *host_out, int n_substeps);
+
+/* ---- per-kernel timing (the reference's PROFILE_GPU stage timers,
+ * Diffusion.cu:1908-1912, as CUDA events) ---------------------------------
+ * When enabled, every launch of this world is bracketed by CUDA events on
+ * its stream.  vfd_read_profile synchronises, returns per kernel kind
+ * (0 = x pass, 1 = y pass, 2 = z pass, 3 = source deposit) the summed
+ * milliseconds and launch counts since the last read, and resets them. */
+vfd_status vfd_world_set_profiling(vfd_world *w, int enable);
+vfd_status vfd_read_profile(vfd_world *w, double *ms4, int64_t *launches4);
+
+/* ---- diagnostics ------------------------------------------------------ */
+const char *vfd_status_string(vfd_status s);
+/* Last error message of this world (or of the last failed create when
+ * w == NULL, per calling thread).  Never NULL. */
+const char *vfd_last_error(const vfd_world *w);
+/* Number of kernels this library launched since load (all worlds). */
+uint64_t vfd_kernel_launch_count(void);
+
+/* ---- deterministic synthetic inputs (workload generator) -------------
+ * Counter-based splitmix64 stream keyed by (seed, world, field, stream):
+ * field values uniform in [lo, hi); sources = n voxels drawn uniformly with
+ * replacement, strengths lognormal(mu, sigma) through FP64 Box-Muller. */
+vfd_status vfd_synth_field(uint64_t seed, int world, int field, float lo, float hi,
+                           float *out, size_t n);
+vfd_status vfd_synth_sources(uint64_t seed, int world, int field, int64_t n,
+                             int64_t n_voxels, double mu, double sigma,
+                             int32_t *idx, float *amt);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VFD_H_ */

@@ -1,0 +1,101 @@
+// ref_replay.cu -- replays the reference's per-field GPU diffusion with the
+// reference's OWN kernels (src/Diffusion/convolutionFFT.cu, compiled from the
+// reference tree by oracle/Makefile) and cuFFT, in the call order of
+// computeKernelSpectrum3D (Diffusion.cu:1533-1619) and fftDiffuse3D
+// (Diffusion.cu:1622-1934):
+//   memset pad; padDataConstantVF3D; cufftExecR2C; modulateAndNormalize3D
+//   (padding 1, scale 1/(fftD*fftH*fftW)); cufftExecC2R; unpadResult3D.
+//
+// TEST INFRASTRUCTURE ONLY: it pins the oracle and the product against the
+// reference's real GPU path on a B200.  Never linked into libvfd.so.
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdio.h>
+
+extern "C" void padKernel3D(float *d_Dst, float *d_Src, int fftD, int fftH, int fftW, int kernelD,
+                            int kernelH, int kernelW, int kernelZ, int kernelY, int kernelX);
+extern "C" void padDataConstantVF3D(float *d_Dst, float *d_Src, int fftD, int fftH, int fftW, int dataD,
+                                    int dataH, int dataW, int kernelD, int kernelH, int kernelW,
+                                    int kernelZ, int kernelY, int kernelX, int epiBoundary,
+                                    float baseChem);
+extern "C" void modulateAndNormalize3D(float2 *d_Dst, float2 *d_Src, int fftD, int fftH, int fftW,
+                                       int padding);
+extern "C" void unpadResult3D(float *d_Dst, float *d_Src, int dataD, int dataH, int dataW, int fftD,
+                              int fftH, int fftW);
+
+#define RR_CHECK(x)                                                                    \
+    do {                                                                               \
+        cudaError_t e_ = (x);                                                          \
+        if (e_ != cudaSuccess) {                                                       \
+            snprintf(g_err, sizeof(g_err), "%s: %s", #x, cudaGetErrorString(e_));      \
+            rc = -1;                                                                   \
+            goto done;                                                                 \
+        }                                                                              \
+    } while (0)
+#define RR_CUFFT(x)                                                                    \
+    do {                                                                               \
+        cufftResult r_ = (x);                                                          \
+        if (r_ != CUFFT_SUCCESS) {                                                     \
+            snprintf(g_err, sizeof(g_err), "%s: cufft error %d", #x, (int)r_);         \
+            rc = -2;                                                                   \
+            goto done;                                                                 \
+        }                                                                              \
+    } while (0)
+
+static char g_err[512] = "";
+
+extern "C" const char *ref_replay_error(void) { return g_err; }
+
+// One field: h_in (D*H*W, x fastest) -> h_out, kernel window h_win
+// (kD*kH*kW, centre kZ,kY,kX) on an fftD*fftH*fftW grid.
+extern "C" int ref_replay_fft_diffuse3d(const float *h_in, float *h_out, int D, int H, int W, int fftD,
+                                        int fftH, int fftW, const float *h_win, int kD, int kH, int kW,
+                                        int kZ, int kY, int kX, int epi, float baseChem)
+{
+    int rc = 0;
+    float *d_data = nullptr, *d_win = nullptr, *d_pk = nullptr, *d_pad = nullptr;
+    float2 *d_ks = nullptr, *d_ds = nullptr;
+    cufftHandle fwd = 0, inv = 0;
+    bool have_fwd = false, have_inv = false;
+    const size_t dsz = (size_t)D * H * W, fsz = (size_t)fftD * fftH * fftW;
+    const size_t ssz = (size_t)fftD * fftH * (fftW / 2 + 1);
+    const size_t wsz = (size_t)kD * kH * kW;
+    RR_CHECK(cudaMalloc(&d_data, dsz * sizeof(float)));
+    RR_CHECK(cudaMalloc(&d_win, wsz * sizeof(float)));
+    RR_CHECK(cudaMalloc(&d_pk, fsz * sizeof(float)));
+    RR_CHECK(cudaMalloc(&d_pad, fsz * sizeof(float)));
+    RR_CHECK(cudaMalloc(&d_ks, ssz * sizeof(float2)));
+    RR_CHECK(cudaMalloc(&d_ds, ssz * sizeof(float2)));
+    RR_CHECK(cudaMemcpy(d_data, h_in, dsz * sizeof(float), cudaMemcpyHostToDevice));
+    RR_CHECK(cudaMemcpy(d_win, h_win, wsz * sizeof(float), cudaMemcpyHostToDevice));
+    RR_CUFFT(cufftPlan3d(&fwd, fftD, fftH, fftW, CUFFT_R2C));
+    have_fwd = true;
+    RR_CUFFT(cufftPlan3d(&inv, fftD, fftH, fftW, CUFFT_C2R));
+    have_inv = true;
+    // kernel spectrum (computeKernelSpectrum3D)
+    RR_CHECK(cudaMemset(d_pk, 0, fsz * sizeof(float)));
+    padKernel3D(d_pk, d_win, fftD, fftH, fftW, kD, kH, kW, kZ, kY, kX);
+    RR_CHECK(cudaGetLastError());
+    RR_CUFFT(cufftExecR2C(fwd, (cufftReal *)d_pk, (cufftComplex *)d_ks));
+    // fftDiffuse3D
+    RR_CHECK(cudaMemset(d_pad, 0, fsz * sizeof(float)));
+    padDataConstantVF3D(d_pad, d_data, fftD, fftH, fftW, D, H, W, kD, kH, kW, kZ, kY, kX, epi, baseChem);
+    RR_CHECK(cudaGetLastError());
+    RR_CUFFT(cufftExecR2C(fwd, (cufftReal *)d_pad, (cufftComplex *)d_ds));
+    modulateAndNormalize3D(d_ds, d_ks, fftD, fftH, fftW, 1);
+    RR_CHECK(cudaGetLastError());
+    RR_CUFFT(cufftExecC2R(inv, (cufftComplex *)d_ds, (cufftReal *)d_pad));
+    unpadResult3D(d_data, d_pad, D, H, W, fftD, fftH, fftW);
+    RR_CHECK(cudaGetLastError());
+    RR_CHECK(cudaMemcpy(h_out, d_data, dsz * sizeof(float), cudaMemcpyDeviceToHost));
+done:
+    if (have_fwd) cufftDestroy(fwd);
+    if (have_inv) cufftDestroy(inv);
+    cudaFree(d_data);
+    cudaFree(d_win);
+    cudaFree(d_pk);
+    cudaFree(d_pad);
+    cudaFree(d_ks);
+    cudaFree(d_ds);
+    return rc;
+}

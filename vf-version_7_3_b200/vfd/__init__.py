@@ -1,0 +1,254 @@
+"""ctypes binding of libvfd.so (include/vfd.h) for tests and benchmarks.
+
+The library is the product: every call here goes through its C ABI.  There
+is no Python or CPU fallback -- importing this module raises if libvfd.so
+is missing, and world creation raises if no CUDA device is visible.
+
+The `World` class mirrors the reference's diffusion surface
+(src/Diffusion/Diffuser.h:24-70, Diffuser::diffuseChemGPU and the
+WHChemical update it feeds): per-world fields resident on the device, one
+`tick()` per simulation tick, `diffuse_host()` for the reference's
+host-buffer-in / host-buffer-out contract.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libvfd.so")
+
+PAD_ZERO = 0
+PAD_CONSTANT_VF = 1
+
+STATUS = {
+    0: "VFD_OK", 1: "VFD_ERR_INVALID_ARG", 2: "VFD_ERR_OUT_OF_MEMORY",
+    3: "VFD_ERR_BUDGET", 4: "VFD_ERR_CUDA", 5: "VFD_ERR_TIMEOUT",
+    6: "VFD_ERR_DEVICE_FAULT", 7: "VFD_ERR_NOT_SUPPORTED", 8: "VFD_ERR_NO_DEVICE",
+}
+
+# Every symbol include/vfd.h declares (checked by the CPU test suite).
+EXPORTED = [
+    "vfd_world_create", "vfd_world_destroy", "vfd_world_fft_dims",
+    "vfd_world_device_bytes", "vfd_upload_field", "vfd_download_field",
+    "vfd_field_device_ptr", "vfd_set_sources", "vfd_tick", "vfd_read_mass",
+    "vfd_diffuse_host", "vfd_status_string", "vfd_last_error",
+    "vfd_kernel_launch_count", "vfd_synth_field", "vfd_synth_sources",
+    "vfd_world_set_profiling", "vfd_read_profile",
+]
+
+
+class VfdError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class FieldParams(C.Structure):
+    _fields_ = [("sigma", C.c_double * 3), ("radius", C.c_int * 3),
+                ("decay_rate", C.c_double), ("baseline", C.c_float)]
+
+
+class WorldDesc(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("n_fields", C.c_int), ("fields", C.POINTER(FieldParams)),
+                ("pad_mode", C.c_int), ("epi_boundary", C.c_int),
+                ("fft", C.c_int * 3)]
+
+
+class Mass(C.Structure):
+    _fields_ = [("input_sum", C.c_double), ("leaked", C.c_double * 3),
+                ("conv_sum", C.c_double), ("total", C.c_double),
+                ("sources", C.c_double), ("reserved", C.c_double)]
+
+    def as_dict(self):
+        return {"input_sum": self.input_sum, "leaked": list(self.leaked),
+                "conv_sum": self.conv_sum, "total": self.total,
+                "sources": self.sources}
+
+
+def load(path=LIB_PATH):
+    if not os.path.exists(path):
+        raise ImportError(f"libvfd.so not built at {path}; run `make` in "
+                          f"{os.path.dirname(path)}/.. or __graft_entry__.build()")
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    lib.vfd_world_create.argtypes = [C.POINTER(WorldDesc), C.c_int, C.POINTER(P)]
+    lib.vfd_world_destroy.argtypes = [P]
+    lib.vfd_world_fft_dims.argtypes = [P, C.POINTER(C.c_int)]
+    lib.vfd_world_device_bytes.argtypes = [P, C.POINTER(C.c_size_t)]
+    lib.vfd_upload_field.argtypes = [P, C.c_int, P, P]
+    lib.vfd_download_field.argtypes = [P, C.c_int, P, P]
+    lib.vfd_field_device_ptr.argtypes = [P, C.c_int, C.POINTER(P)]
+    lib.vfd_set_sources.argtypes = [P, C.c_int, P, P, C.c_int64]
+    lib.vfd_tick.argtypes = [P, C.c_int, P]
+    lib.vfd_read_mass.argtypes = [P, C.POINTER(Mass), P]
+    lib.vfd_diffuse_host.argtypes = [P, C.POINTER(P), C.POINTER(P), C.c_int]
+    lib.vfd_world_set_profiling.argtypes = [P, C.c_int]
+    lib.vfd_read_profile.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    lib.vfd_status_string.argtypes = [C.c_int]
+    lib.vfd_status_string.restype = C.c_char_p
+    lib.vfd_last_error.argtypes = [P]
+    lib.vfd_last_error.restype = C.c_char_p
+    lib.vfd_kernel_launch_count.argtypes = []
+    lib.vfd_kernel_launch_count.restype = C.c_uint64
+    lib.vfd_synth_field.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_float, C.c_float, P, C.c_size_t]
+    lib.vfd_synth_sources.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int64, C.c_int64,
+                                      C.c_double, C.c_double, P, P]
+    for name in EXPORTED:
+        if name not in ("vfd_status_string", "vfd_last_error", "vfd_kernel_launch_count"):
+            getattr(lib, name).restype = C.c_int
+    return lib
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = load()
+    return _lib
+
+
+def _check(status, world_ptr=None):
+    if status != 0:
+        msg = lib().vfd_last_error(world_ptr).decode()
+        raise VfdError(status, msg)
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+def synth_field(seed, world, field, shape_zyx, lo=0.0, hi=1e-3):
+    out = np.empty(shape_zyx, dtype=np.float32)
+    _check(lib().vfd_synth_field(seed, world, field, lo, hi, _ptr(out), out.size))
+    return out
+
+
+def synth_sources(seed, world, field, n, n_voxels, mu=-6.0, sigma=1.0):
+    idx = np.empty(n, dtype=np.int32)
+    amt = np.empty(n, dtype=np.float32)
+    _check(lib().vfd_synth_sources(seed, world, field, n, n_voxels, mu, sigma,
+                                   _ptr(idx), _ptr(amt)))
+    return idx, amt
+
+
+def field_params(sigma, decay_rate, radius=None, baseline=0.0):
+    """sigma: scalar or (sx, sy, sz); radius: None (ceil(3 sigma)) or int / triple."""
+    p = FieldParams()
+    s = [float(sigma)] * 3 if np.isscalar(sigma) else [float(v) for v in sigma]
+    r = [0, 0, 0] if radius is None else ([int(radius)] * 3 if np.isscalar(radius)
+                                         else [int(v) for v in radius])
+    for a in range(3):
+        p.sigma[a] = s[a]
+        p.radius[a] = r[a]
+    p.decay_rate = float(decay_rate)
+    p.baseline = float(baseline)
+    return p
+
+
+class World:
+    """One world of `n_fields` fields on an nx*ny*nz grid (x fastest)."""
+
+    def __init__(self, nx, ny, nz, params, pad_mode=PAD_ZERO, epi_boundary=0,
+                 fft=(0, 0, 0), device=0):
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.nf = len(params)
+        self._params = (FieldParams * self.nf)(*params)
+        d = WorldDesc()
+        d.nx, d.ny, d.nz, d.n_fields = nx, ny, nz, self.nf
+        d.fields = C.cast(self._params, C.POINTER(FieldParams))
+        d.pad_mode, d.epi_boundary = pad_mode, epi_boundary
+        for a in range(3):
+            d.fft[a] = int(fft[a])
+        h = C.c_void_p()
+        _check(lib().vfd_world_create(C.byref(d), device, C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().vfd_world_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def shape(self):
+        return (self.nz, self.ny, self.nx)
+
+    def fft_dims(self):
+        a = (C.c_int * 3)()
+        _check(lib().vfd_world_fft_dims(self._h, a), self._h)
+        return tuple(a)
+
+    def device_bytes(self):
+        b = C.c_size_t()
+        _check(lib().vfd_world_device_bytes(self._h, C.byref(b)), self._h)
+        return b.value
+
+    def upload(self, field, arr, stream=None):
+        a = np.ascontiguousarray(arr, dtype=np.float32)
+        assert a.size == self.nx * self.ny * self.nz
+        # pageable source: the call returns once the buffer has been staged
+        _check(lib().vfd_upload_field(self._h, field, _ptr(a), stream), self._h)
+        return a
+
+    def download(self, field, out=None, stream=None):
+        if out is None:
+            out = np.empty(self.shape, dtype=np.float32)
+        _check(lib().vfd_download_field(self._h, field, _ptr(out), stream), self._h)
+        return out
+
+    def device_ptr(self, field):
+        p = C.c_void_p()
+        _check(lib().vfd_field_device_ptr(self._h, field, C.byref(p)), self._h)
+        return p.value
+
+    def set_sources(self, field, idx, amt):
+        i = np.ascontiguousarray(idx, dtype=np.int32)
+        a = np.ascontiguousarray(amt, dtype=np.float32)
+        assert i.size == a.size
+        _check(lib().vfd_set_sources(self._h, field, _ptr(i), _ptr(a), i.size), self._h)
+
+    def tick(self, n_substeps=1, stream=None):
+        _check(lib().vfd_tick(self._h, n_substeps, stream), self._h)
+
+    def mass(self, stream=None):
+        m = (Mass * self.nf)()
+        _check(lib().vfd_read_mass(self._h, m, stream), self._h)
+        return [x.as_dict() for x in m]
+
+    def set_profiling(self, enable=True):
+        _check(lib().vfd_world_set_profiling(self._h, int(bool(enable))), self._h)
+
+    def read_profile(self):
+        """{kind: (ms_total, launches)} for kinds x, y, z, deposit since the last read."""
+        ms = (C.c_double * 4)()
+        n = (C.c_int64 * 4)()
+        _check(lib().vfd_read_profile(self._h, ms, n), self._h)
+        return {k: (ms[i], n[i]) for i, k in enumerate(("x", "y", "z", "deposit"))}
+
+    def diffuse_host(self, host_in, host_out, n_substeps=1):
+        ins = (C.c_void_p * self.nf)(*[a.ctypes.data for a in host_in])
+        outs = (C.c_void_p * self.nf)(*[a.ctypes.data for a in host_out])
+        _check(lib().vfd_diffuse_host(self._h, ins, outs, n_substeps), self._h)
+
+
+def launch_count():
+    return int(lib().vfd_kernel_launch_count())
