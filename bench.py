@@ -176,19 +176,128 @@ def run_reference(args, c):
     print(json.dumps(line), flush=True)
 
 
+def run_cfg2(args):
+    """Batched ensemble: 32 uneven worlds x 8 fields, 10 substeps per tick, all
+    fields of all worlds in one launch per axis pass, tick replayed as a CUDA
+    graph.  Beside it: the same worlds through the plain per-field path
+    (VFD_METHOD_PLAIN: unfused kernels, one field at a time, no graph)."""
+    import torch
+
+    import vfd
+    from vfd import configs
+    dev = 0
+    torch.cuda.set_device(dev)
+    c = configs.CFG2
+    specs = configs.cfg2_worlds(c["n_worlds"], c["seed"])
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+
+    def build(method):
+        ws = []
+        for sp in specs:
+            nx, ny, nz = sp["grid"]
+            params = [vfd.field_params(s_, d_) for s_, d_ in zip(sp["sigma"], sp["decay"])]
+            w = vfd.World(nx, ny, nz, params, method=method)
+            for f, (u, idx, amt) in enumerate(configs.field_inputs(c["seed"], sp["world"], sp["grid"],
+                                                                     sp["n_sources"])):
+                w.upload(f, u)
+                w.set_sources(f, idx, amt)
+            ws.append(w)
+        return ws
+
+    vox = sum(configs.voxels(sp["grid"]) for sp in specs) * 8 * c["substeps"]
+    worlds = build(vfd.METHOD_SEPARABLE)
+    batch = vfd.Batch(worlds)
+    for _ in range(args.warmup):
+        batch.tick(c["substeps"], stream=sh)
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    l0 = vfd.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        batch.tick(c["substeps"], stream=sh)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    launches = vfd.launch_count() - l0
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    value = vox * args.steps / (ms / 1e3)
+    # the same worlds ticked one world at a time (separable kernels, no batch, no graph)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for w in worlds:
+        w.tick(c["substeps"], stream=sh)
+    t0.record(stream)
+    for w in worlds:
+        w.tick(c["substeps"], stream=sh)
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    unbatched = vox / (t0.elapsed_time(t1) / 1e3)
+    batch.close()
+    for w in worlds:
+        w.close()
+    # plain per-field path, one world at a time (bounded: 1 tick)
+    plain_ms = 0.0
+    for sp in specs:
+        nx, ny, nz = sp["grid"]
+        params = [vfd.field_params(s_, d_) for s_, d_ in zip(sp["sigma"], sp["decay"])]
+        w = vfd.World(nx, ny, nz, params, method=vfd.METHOD_PLAIN)
+        for f, (u, idx, amt) in enumerate(configs.field_inputs(c["seed"], sp["world"], sp["grid"],
+                                                                 sp["n_sources"])):
+            w.upload(f, u)
+            w.set_sources(f, idx, amt)
+        w.tick(1, stream=sh)
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        w.tick(c["substeps"], stream=sh)
+        p1.record(stream)
+        torch.cuda.synchronize(dev)
+        plain_ms += p0.elapsed_time(p1)
+        w.close()
+    plain = vox / (plain_ms / 1e3)
+    alg = 24.0 * vox / c["substeps"] * c["substeps"] / 8.0  # bytes: 24 B per voxel-step
+    peak, kind = peaks()
+    achieved = 24.0 * vox * args.steps / (ms / 1e3) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded counter-based generator)",
+            "config": {"workload": "batched ensemble: 32 worlds drawn from {96x64x64, 128x96x96, "
+                                   "192x128x128, 256x128x192} x 8 fields, 10 substeps per step, "
+                                   "500 sources/field, sigma and decay x U[0.5, 2], seed 0",
+                       "worlds": [list(sp["grid"]) for sp in specs],
+                       "l2": "inputs larger than L2"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": "whole step, 24 B per voxel-step (3 axis passes x 8 B)",
+                         "peak_source": f"{kind} hbm_gbs"},
+            "plain_gpu": {"value": plain, "unit": METRIC,
+                          "what": "VFD_METHOD_PLAIN: unfused pad/R2C/C2C/multiply/C2C/C2R/crop kernels, "
+                                  "one field per launch sequence, no graph"},
+            "unbatched_separable": {"value": unbatched, "unit": METRIC},
+            "batched_over_plain": value / plain,
+            "gpu_launches": launches, "clocks": clk}
+    del alg
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="vfd", choices=["vfd", "reference"])
-    ap.add_argument("--config", default="cfg1", choices=["cfg0", "cfg1", "cfg4"])
+    ap.add_argument("--config", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg4"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-fields", type=int, default=2,
                     help="fields in the CPU-baseline sample (1 substep each)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
-    c = cfg_by_name(args.config)
+    if args.config == "cfg2" and args.impl == "vfd":
+        run_cfg2(args)
+        return
+    c = cfg_by_name(args.config if args.config != "cfg2" else "cfg1")
     if args.impl == "reference":
         run_reference(args, c)
         return
@@ -280,6 +389,7 @@ def main():
     world.diffuse_host(host_in, host_out, c["substeps"])
     barrier()
     torch.cuda.synchronize(dev)
+    args.e2e_steps = max(1, args.e2e_steps)
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
         for f, (u, idx, amt) in enumerate(ins):

@@ -56,6 +56,25 @@ typedef enum vfd_pad_mode {
     VFD_PAD_CONSTANT_VF = 1
 } vfd_pad_mode;
 
+/* How a substep's 3D FFT convolution is evaluated.
+ * VFD_METHOD_SEPARABLE (default): the Gaussian spectrum is separable, so the
+ *   3D transform factorises into three fused per-axis FFT convolutions
+ *   (forward FFT, multiply, inverse FFT, crop) with one HBM read and write of
+ *   the field per axis.
+ * VFD_METHOD_FFT3D: the full 3D R2C FFT, multiply by a stored 3D spectrum,
+ *   C2R, with the padding rule fused into the R2C pass, the multiply fused
+ *   between the forward and inverse z transforms and the crop fused into the
+ *   C2R pass; zero padding and cropped outputs are pruned.  Any kernel
+ *   (vfd_set_window) -- the reference's stencil-power window included.
+ * VFD_METHOD_PLAIN: the same 3D transform as unfused per-field kernels in the
+ *   reference's order (pad, R2C, C2C y, C2C z, multiply, C2C z, C2C y, C2R,
+ *   crop) on the full FFT grid -- fftDiffuse3D's structure, Diffusion.cu:1622-1934. */
+typedef enum vfd_method {
+    VFD_METHOD_SEPARABLE = 0,
+    VFD_METHOD_FFT3D = 1,
+    VFD_METHOD_PLAIN = 2
+} vfd_method;
+
 /* Per-field diffusion parameters.
  * Kernel: normalised sampled Gaussian exp(-j^2/(2 sigma^2)) per axis,
  * truncated to [-radius, radius] on each axis and normalised in FP64 (the
@@ -81,6 +100,7 @@ typedef struct vfd_world_desc {
     int pad_mode;                   /* vfd_pad_mode                       */
     int epi_boundary;               /* constant-VF x bound (rightWallIndex) */
     int fft[3];                     /* FFT length per axis; 0 = planner   */
+    int method;                     /* vfd_method                         */
 } vfd_world_desc;
 
 typedef struct vfd_world vfd_world;
@@ -120,6 +140,17 @@ vfd_status vfd_field_device_ptr(vfd_world *w, int field, float **dptr);
 vfd_status vfd_set_sources(vfd_world *w, int field, const int32_t *idx,
                            const float *amt, int64_t n);
 
+/* ---- reference-mode kernel (computeKernelSpectrum3D, Diffusion.cu:1533-1619)
+ * Replaces field `field`'s Gaussian by a dense real window w (kd*kh*kw,
+ * x fastest) whose centre (cx, cy, cz) is wrapped to index 0 like
+ * padKernel3D (convolutionFFT.cuh:402-445); its 3D spectrum is computed on the
+ * device with this library's FFT.  Worlds created with VFD_METHOD_FFT3D or
+ * VFD_METHOD_PLAIN only (VFD_ERR_NOT_SUPPORTED otherwise).  The window must
+ * fit the FFT grid: the planner grid covers n + max(radius); pass explicit
+ * fft lengths >= n + window half-width for wider windows. */
+vfd_status vfd_set_window(vfd_world *w, int field, const float *window, int kw, int kh, int kd,
+                          int cx, int cy, int cz);
+
 /* ---- one tick: n_substeps diffusion substeps of every field, then the
  * registered sources are deposited and the FP64 totals are formed.
  * Replaces fftDiffuse3D (Diffusion.cu:1622-1934) for every chemical plus
@@ -138,6 +169,20 @@ vfd_status vfd_read_mass(vfd_world *w, vfd_mass *out, void *stream);
  * Synchronous: returns when host_out holds the result. */
 vfd_status vfd_diffuse_host(vfd_world *w, const float *const *host_in,
                             float *const *host_out, int n_substeps);
+
+/* ---- batched ensembles (sensitivity-analysis ensembles of many worlds) --
+ * A batch references (does not own) n_worlds worlds on one device; they
+ * must outlive it.  vfd_batch_tick is vfd_tick on every world, but every
+ * field of every world goes through one kernel launch per axis pass per
+ * substep, and the whole tick is captured once into a CUDA graph and
+ * replayed (re-captured when n_substeps or a world's sources change).
+ * The reference runs worlds one at a time and its chemicals one at a time
+ * (Diffuser.cpp:300-341); it has no batched form. */
+typedef struct vfd_batch vfd_batch;
+vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **out);
+vfd_status vfd_batch_tick(vfd_batch *b, int n_substeps, void *stream);
+vfd_status vfd_batch_destroy(vfd_batch *b);
+const char *vfd_batch_last_error(const vfd_batch *b);
 
 /* ---- per-kernel timing (the reference's PROFILE_GPU stage timers,
  * Diffusion.cu:1908-1912, as CUDA events) ---------------------------------

@@ -1,0 +1,151 @@
+"""GPU tests of the general 3D FFT convolution (VFD_METHOD_FFT3D fused and
+pruned, VFD_METHOD_PLAIN unfused in fftDiffuse3D's order) and of
+reference-mode windows (vfd_set_window), against the FP64 oracle and -- when
+oracle/_ref is built -- against the reference's own kernels + cuFFT."""
+import numpy as np
+import pytest
+
+import oracle
+import vfd
+from vfd import configs
+
+pytestmark = pytest.mark.gpu
+
+REL_L2 = 1e-5
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
+
+
+def run(method, grid, sig, dec, ins, substeps=1, pad_mode=0, epi=0, base=None, fft=(0, 0, 0), windows=None):
+    nx, ny, nz = grid
+    params = [vfd.field_params(s, d, baseline=(base[f] if base else 0.0)) for f, (s, d) in enumerate(zip(sig, dec))]
+    with vfd.World(nx, ny, nz, params, pad_mode=pad_mode, epi_boundary=epi, fft=fft, method=method) as w:
+        if windows:
+            for f, (win, c) in windows.items():
+                w.set_window(f, win, c)
+        for f, (u, idx, amt) in enumerate(ins):
+            w.upload(f, u)
+            w.set_sources(f, idx, amt)
+        w.tick(substeps)
+        outs = [w.download(f) for f in range(len(ins))]
+        return outs, w.mass(), w.fft_dims()
+
+
+@pytest.mark.parametrize("method", [vfd.METHOD_FFT3D, vfd.METHOD_PLAIN])
+@pytest.mark.parametrize("grid", [(64, 64, 32), (37, 20, 13)])
+def test_gaussian_general_methods_against_oracle(gpu, method, grid):
+    nx, ny, nz = grid
+    sig = [1.2, (0.7, 1.4, 1.0)]
+    dec = [0.05, 0.02]
+    ins = configs.field_inputs(0, 3, grid, 100, n_fields=2)
+    outs, mass, _ = run(method, grid, sig, dec, ins, substeps=2)
+    for f, (u, idx, amt) in enumerate(ins):
+        ref = oracle.tick(u, sig[f], dec[f], 2, idx, amt)
+        assert rel_l2(outs[f], ref) <= REL_L2, (method, grid, f)
+        s = outs[f].astype(np.float64).sum()
+        assert abs(mass[f]["total"] - s) <= 1e-6 * s
+
+
+@pytest.mark.parametrize("method", [vfd.METHOD_FFT3D, vfd.METHOD_PLAIN])
+def test_constant_vf_general_methods(gpu, method):
+    grid = (48, 40, 36)
+    nx, ny, nz = grid
+    sig, dec, base = [1.2, 0.9], [0.05, 0.0], [4e-4, 7e-4]
+    ins = [(vfd.synth_field(5, 0, f, (nz, ny, nx)), np.zeros(0, np.int32), np.zeros(0, np.float32))
+           for f in range(2)]
+    outs, _, _ = run(method, grid, sig, dec, ins, pad_mode=1, epi=37, base=base)
+    for f, (u, idx, amt) in enumerate(ins):
+        ref = oracle.tick(u, sig[f], dec[f], 1, idx, amt, b=float(np.float32(base[f])), pad_mode=1, epi=37)
+        assert rel_l2(outs[f], ref) <= REL_L2, (method, f)
+
+
+def test_plain_mass_identity(gpu):
+    grid = (40, 30, 20)
+    ins = configs.field_inputs(1, 0, grid, 0, n_fields=1)
+    outs, mass, _ = run(vfd.METHOD_PLAIN, grid, [1.5], [0.0], ins)
+    m = mass[0]
+    # full-grid conservation of the circular convolution
+    assert abs(m["input_sum"] - m["conv_sum"] - sum(m["leaked"])) <= 1e-6 * m["input_sum"]
+
+
+def _stencil_window(lam, n, R):
+    return oracle.stencil_power(lam, 0.0, n, R)
+
+
+@pytest.mark.parametrize("method", [vfd.METHOD_FFT3D, vfd.METHOD_PLAIN])
+def test_reference_mode_stencil_window(gpu, method):
+    """Reference-mode kernel: the 7-point stencil (lambda = 0.1333) to the
+    power 30, truncated to a 21^3 window, as a dense window."""
+    grid = (40, 36, 30)
+    nx, ny, nz = grid
+    R = 10
+    w = _stencil_window(0.1333, 30, R)
+    ins = [(vfd.synth_field(2, 0, 0, (nz, ny, nx)), np.zeros(0, np.int32), np.zeros(0, np.float32))]
+    fft = (56, 48, 42)  # 7-smooth, even x, >= n + R on every axis
+    outs, mass, dims = run(method, grid, [1.0], [0.0], ins, fft=fft,
+                           windows={0: (w.astype(np.float32), (R, R, R))})
+    v = ins[0][0].astype(np.float64)
+    ref = oracle.conv_direct3d(v, w.astype(np.float32).astype(np.float64), (R, R, R))
+    assert rel_l2(outs[0], ref) <= REL_L2
+
+
+def test_three_methods_agree_cfg0(gpu):
+    c = configs.CFG0
+    ins = configs.field_inputs(c["seed"], 0, c["grid"], c["n_sources"], n_fields=3)
+    res = [run(m, c["grid"], c["sigma"][:3], c["decay"][:3], ins)[0]
+           for m in (vfd.METHOD_SEPARABLE, vfd.METHOD_FFT3D, vfd.METHOD_PLAIN)]
+    for f in range(3):
+        assert rel_l2(res[1][f], res[0][f]) <= 2e-6
+        assert rel_l2(res[2][f], res[0][f]) <= 2e-6
+
+
+def test_window_rejected_for_separable(gpu):
+    with vfd.World(16, 16, 16, [vfd.field_params(1.0, 0.0)]) as w:
+        with pytest.raises(vfd.VfdError) as e:
+            w.set_window(0, np.ones((3, 3, 3), np.float32) / 27)
+        assert e.value.status == 7
+
+
+@pytest.mark.skipif(not oracle.ref_replay_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("kind", ["gaussian", "stencil"])
+def test_against_reference_kernels_and_cufft(gpu, kind):
+    """The reference's own padDataConstantVF3D / modulateAndNormalize3D /
+    unpadResult3D + cuFFT (fftDiffuse3D's order) on the same field, window
+    and FFT grid as this library's general and separable paths."""
+    grid = (48, 40, 36)
+    nx, ny, nz = grid
+    base, epi = 3e-4, 40
+    u = vfd.synth_field(11, 0, 0, (nz, ny, nx))
+    if kind == "gaussian":
+        sig = 1.3
+        r = configs.radius(sig)
+        t = oracle.gauss_taps(sig, r)
+        win = np.einsum("z,y,x->zyx", t, t, t).astype(np.float32)
+        R = r
+    else:
+        R = 8
+        win = _stencil_window(0.1333, 20, R).astype(np.float32)
+        sig = 1.0
+    fft = (64, 48, 48)
+    ins = [(u, np.zeros(0, np.int32), np.zeros(0, np.float32))]
+    ref = oracle.ref_replay(u, fft, win, (R, R, R), epi, base)
+    outs, _, _ = run(vfd.METHOD_FFT3D, grid, [sig], [0.0], ins, pad_mode=1, epi=epi, base=[base], fft=fft,
+                     windows={0: (win, (R, R, R))})
+    assert rel_l2(outs[0], ref) <= REL_L2
+    outs_p, _, _ = run(vfd.METHOD_PLAIN, grid, [sig], [0.0], ins, pad_mode=1, epi=epi, base=[base], fft=fft,
+                       windows={0: (win, (R, R, R))})
+    assert rel_l2(outs_p[0], ref) <= REL_L2
+    # oracle (FP64) vs the reference's FP32 cuFFT path
+    v = u.astype(np.float64) - np.float32(base)
+    mask = np.zeros_like(v, bool)
+    mask[1:nz - 1, 1:ny - 1, 1:epi] = True
+    v[~mask] = 0.0
+    o = oracle.conv_direct3d(v, win.astype(np.float64), (R, R, R)) + np.float32(base) * win.astype(np.float64).sum()
+    assert rel_l2(ref, o) <= REL_L2
+    if kind == "gaussian":
+        sep, _, _ = run(vfd.METHOD_SEPARABLE, grid, [sig], [0.0], ins, pad_mode=1, epi=epi, base=[base])
+        assert rel_l2(sep[0], ref) <= REL_L2

@@ -23,8 +23,9 @@ enum PassKind { PASS_X = 0, PASS_Y = 1, PASS_Z = 2 };
 // One (field, axis) pass.  Real lines of the field are addressed as
 //   base + line*line_stride + outer*outer_stride + pos*pos_stride,
 // line in [0, nlines), outer in [0, nouter), pos in [0, n).
-// A tile takes 2*NL consecutive lines of one outer index; line l0+q goes to
-// complex line q % NL, plane q / NL (0 = real, 1 = imaginary).
+// A tile takes 2*NL consecutive lines of one outer index (NL of the kernel
+// variant the launch uses); line l0+q goes to complex line q % NL, real part
+// for q < NL, imaginary part otherwise.
 struct AxisJob {
     float *data;
     const float2 *tw;     // F twiddles exp(-2 pi i m / F), FP64-generated

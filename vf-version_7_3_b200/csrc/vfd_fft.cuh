@@ -2,12 +2,12 @@
 //
 // Replaces cuFFT's 3D R2C / C2R (src/Diffusion/Diffusion.cu:1814, 1842 in the
 // reference) on the product path.  Lines of one axis are transformed in
-// batches of NL complex lines held in shared memory as two split planes
-// (re, im) laid out [position][line] with an odd line stride LS, so that
-//   * a warp's lanes address different lines of the same position during
-//     butterflies (conflict-free, twiddles uniform across the lines), and
-//   * transposing loads (32 consecutive positions of one line) hit 32
-//     distinct banks.
+// batches of NL complex lines held in shared memory as interleaved complex
+// values laid out [position][line] with an odd line stride LS = NL + 1, so
+// that
+//   * during butterflies each half-warp addresses NL consecutive lines of one
+//     position (conflict-free 64-bit accesses, twiddles uniform per line set),
+//   * transposing loads (one real line per lane) hit distinct banks.
 // Each complex line carries two real lines of the field (real part and
 // imaginary part).  Because the Gaussian heat-kernel spectrum is real and
 // even, multiplying the spectrum of (a + i b) by it convolves a and b
@@ -20,14 +20,18 @@
 
 namespace vfd {
 
-constexpr int NL = 16;          // complex lines per tile (32 real lines)
-constexpr int LS = NL + 1;      // floats per position in one plane
 constexpr int MAX_STAGES = 12;
+constexpr int NL_MAX = 16;      // largest lines-per-tile of any kernel variant
 
+// A mixed-radix plan: F = prod(radix[s]); ns[s] = prod(radix[0..s-1]);
+// ns_magic[s] = ceil(2^21 / ns[s]) gives j / ns = (j * magic) >> 21 exactly
+// for j < 2048 and ns < 1024.
 struct FftPlan {
     int F;
     int nst;
     int radix[MAX_STAGES];
+    int ns[MAX_STAGES];
+    int ns_magic[MAX_STAGES];
 };
 
 __device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
@@ -191,36 +195,34 @@ struct Dft<5, INV> : DftOdd<5, INV> {};
 template <bool INV>
 struct Dft<7, INV> : DftOdd<7, INV> {};
 
-// One radix-R Stockham stage, in place on the split planes.  Thread (line,
-// tj) handles butterflies j = tj, tj + TL, ...  All reads of the stage
-// complete (barrier) before any write.  MAXP bounds the points per thread.
+// One radix-R Stockham stage, in place on the interleaved complex tile.
+// Thread (line, tj) handles butterflies j = tj, tj + TL, ...  All reads of
+// the stage complete (barrier) before any write.  MAXP bounds the points a
+// thread holds; buf is one register buffer shared by all radices.
 //   inputs  a[j + r*M], twiddled by w_F^{(j mod Ns) * r * F/(Ns*R)}
 //   outputs b[(j - j mod Ns)*R + j mod Ns + r*Ns]
-template <int R, int MAXP, int TL, bool INV>
-__device__ __forceinline__ void stockham_stage(float *__restrict__ re, float *__restrict__ im,
-                                               int F, int Ns, int line, int tj,
-                                               const float2 *__restrict__ tw, float2 (&buf)[MAXP])
+template <int R, int MAXP, int TL, int NL, bool INV>
+__device__ __forceinline__ void stockham_stage(float2 *__restrict__ S, int F, int Ns, int magic, int line,
+                                               int tj, const float2 *__restrict__ tw, float2 (&buf)[MAXP])
 {
+    constexpr int LS = NL + 1;
     constexpr int MB = MAXP / R;
     const int M = F / R;
-    const int step = F / (Ns * R);
-    // One register buffer shared by every radix: the stages of a plan then
-    // reuse the same registers instead of each switch case getting its own.
+    const int step = M / Ns;
     float2(*v)[R] = reinterpret_cast<float2(*)[R]>(buf);
 #pragma unroll
     for (int b = 0; b < MB; ++b) {
         const int j = tj + b * TL;
         if (j < M) {
-            const int jm = j % Ns;
+            const int q = (j * magic) >> 21;
+            const int jm = j - q * Ns;
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int p = (j + r * M) * LS + line;
-                v[b][r] = make_float2(re[p], im[p]);
-            }
+            for (int r = 0; r < R; ++r) v[b][r] = S[(j + r * M) * LS + line];
             if (jm != 0) {
+                const int t1 = jm * step;
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
-                    float2 w = tw[jm * r * step];
+                    float2 w = tw[t1 * r];
                     if (INV) w.y = -w.y;
                     v[b][r] = c_mul(v[b][r], w);
                 }
@@ -233,38 +235,31 @@ __device__ __forceinline__ void stockham_stage(float *__restrict__ re, float *__
     for (int b = 0; b < MB; ++b) {
         const int j = tj + b * TL;
         if (j < M) {
-            const int jm = j % Ns;
-            const int d = (j - jm) * R + jm;
+            const int q = (j * magic) >> 21;
+            const int d = q * Ns * (R - 1) + j;  // (j - jm) * R + jm
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int p = (d + r * Ns) * LS + line;
-                re[p] = v[b][r].x;
-                im[p] = v[b][r].y;
-            }
+            for (int r = 0; r < R; ++r) S[(d + r * Ns) * LS + line] = v[b][r];
         }
     }
     __syncthreads();
 }
 
-template <int MAXP, int TL, bool INV>
-__device__ __forceinline__ void fft_lines(float *re, float *im, const FftPlan &pl, int line, int tj,
-                                          const float2 *tw)
+template <int MAXP, int TL, int NL, bool INV>
+__device__ __forceinline__ void fft_lines(float2 *S, const FftPlan &pl, int line, int tj, const float2 *tw)
 {
     float2 buf[MAXP];
-    int Ns = 1;
 #pragma unroll 1
     for (int s = 0; s < pl.nst; ++s) {
-        const int R = pl.radix[s];
+        const int R = pl.radix[s], Ns = pl.ns[s], mg = pl.ns_magic[s];
         switch (R) {
-        case 8: stockham_stage<8, MAXP, TL, INV>(re, im, pl.F, Ns, line, tj, tw, buf); break;
-        case 4: stockham_stage<4, MAXP, TL, INV>(re, im, pl.F, Ns, line, tj, tw, buf); break;
-        case 2: stockham_stage<2, MAXP, TL, INV>(re, im, pl.F, Ns, line, tj, tw, buf); break;
-        case 3: stockham_stage<3, MAXP, TL, INV>(re, im, pl.F, Ns, line, tj, tw, buf); break;
-        case 5: stockham_stage<5, MAXP, TL, INV>(re, im, pl.F, Ns, line, tj, tw, buf); break;
-        case 7: stockham_stage<7, MAXP, TL, INV>(re, im, pl.F, Ns, line, tj, tw, buf); break;
+        case 8: stockham_stage<8, MAXP, TL, NL, INV>(S, pl.F, Ns, mg, line, tj, tw, buf); break;
+        case 4: stockham_stage<4, MAXP, TL, NL, INV>(S, pl.F, Ns, mg, line, tj, tw, buf); break;
+        case 2: stockham_stage<2, MAXP, TL, NL, INV>(S, pl.F, Ns, mg, line, tj, tw, buf); break;
+        case 3: stockham_stage<3, MAXP, TL, NL, INV>(S, pl.F, Ns, mg, line, tj, tw, buf); break;
+        case 5: stockham_stage<5, MAXP, TL, NL, INV>(S, pl.F, Ns, mg, line, tj, tw, buf); break;
+        case 7: stockham_stage<7, MAXP, TL, NL, INV>(S, pl.F, Ns, mg, line, tj, tw, buf); break;
         default: break;
         }
-        Ns *= R;
     }
 }
 

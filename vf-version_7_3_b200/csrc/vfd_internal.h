@@ -15,19 +15,33 @@ struct DepositJob {
     int64_t nvox;     // V, to reject out-of-range voxel indices
 };
 
-// Dynamic shared memory of one axis-pass CTA for FFT length F:
-// two planes of F*LS floats, F twiddles (float2) and F multipliers.
-inline size_t axis_smem_bytes(int F)
+// Dynamic shared memory of one axis-pass CTA for FFT length F and NL lines:
+// F*(NL+1) interleaved complex values, F twiddles (float2), F multipliers.
+inline size_t axis_smem_bytes(int F, int NL)
 {
-    return (size_t)F * LS * 2 * sizeof(float) + (size_t)F * sizeof(float2) + (size_t)F * sizeof(float);
+    return (size_t)F * (NL + 1) * sizeof(float2) + (size_t)F * sizeof(float2) + (size_t)F * sizeof(float);
 }
 inline size_t axis_smem_limit() { return 220 * 1024; }
 
-// Kernel variants (threads per line TL, max points per thread MAXP):
-//   0: (16, 24)  1: (32, 16)  2: (32, 24)  3: (16, 40)  4: (32, 40)
-constexpr int kNumAxisVariants = 5;
-inline int variant_tl(int v) { return (v == 0 || v == 3) ? 16 : 32; }
-inline int variant_maxp(int v) { return v == 0 ? 24 : v == 1 ? 16 : v == 2 ? 24 : 40; }
+// Kernel variants: (index, lines per tile NL, threads per line TL, max points
+// per thread MAXP, min resident blocks per SM for the register budget).
+#define VFD_AXIS_VARIANTS(X) \
+    X(0, 8, 32, 24, 2)       \
+    X(1, 8, 64, 16, 2)       \
+    X(2, 16, 32, 16, 2)      \
+    X(3, 16, 32, 24, 1)      \
+    X(4, 8, 32, 40, 1)       \
+    X(5, 16, 32, 40, 1)
+
+struct AxisVariant {
+    int nl, tl, maxp, minb;
+};
+constexpr AxisVariant kAxisVariants[] = {
+#define VFD_VARIANT_ROW(i, NL, TL, MAXP, MINB) {NL, TL, MAXP, MINB},
+    VFD_AXIS_VARIANTS(VFD_VARIANT_ROW)
+#undef VFD_VARIANT_ROW
+};
+constexpr int kNumAxisVariants = sizeof(kAxisVariants) / sizeof(kAxisVariants[0]);
 
 cudaError_t launch_axis(int variant, const AxisJob *jobs, int njobs, int tiles, int Fmax,
                         cudaStream_t st);

@@ -41,11 +41,19 @@ __device__ __forceinline__ void block_sum_atomic(double v, double *dst, double *
     __syncthreads();
 }
 
-template <int TL, int MAXP>
-__global__ void __launch_bounds__(NL *TL) axis_pass_kernel(const AxisJob *__restrict__ jobs, int njobs)
+// Loads / stores map one real line of the tile to each lane (NR = 2*NL real
+// lines), position groups to the rest of the block, and keep U loads in
+// flight per thread.  Real line rl of the tile is complex line rl % NL,
+// component rl / NL.
+template <int NL, int TL, int MAXP, int MINB>
+__global__ void __launch_bounds__(NL *TL, MINB) axis_pass_kernel(const AxisJob *__restrict__ jobs, int njobs)
 {
     constexpr int NT = NL * TL;
-    extern __shared__ __align__(16) float smem[];
+    constexpr int LS = NL + 1;
+    constexpr int NR = 2 * NL;
+    constexpr int NPG = NT / NR;
+    constexpr int U = 8;
+    extern __shared__ __align__(16) float2 smem2[];
     __shared__ double red[NT / 32];
     __shared__ AxisJob sj;
 
@@ -63,9 +71,9 @@ __global__ void __launch_bounds__(NL *TL) axis_pass_kernel(const AxisJob *__rest
 
     const int F = sj.plan.F;
     const int n = sj.n;
-    float *re = smem;
-    float *im = re + F * LS;
-    float2 *tw = reinterpret_cast<float2 *>(im + F * LS);
+    float2 *S = smem2;
+    float *Sf = reinterpret_cast<float *>(smem2);
+    float2 *tw = S + F * LS;
     float *G = reinterpret_cast<float *>(tw + F);
     for (int i = threadIdx.x; i < F; i += NT) {
         tw[i] = sj.tw[i];
@@ -74,89 +82,143 @@ __global__ void __launch_bounds__(NL *TL) axis_pass_kernel(const AxisJob *__rest
 
     const int local = tile - sj.tile_begin;
     const int outer = local / sj.tiles_per_outer;
-    const int l0 = (local - outer * sj.tiles_per_outer) * (2 * NL);
-    const int nreal = min(2 * NL, sj.nlines - l0);
+    const int l0 = (local - outer * sj.tiles_per_outer) * NR;
+    const int nreal = min(NR, sj.nlines - l0);
     float *base = sj.data + outer * sj.outer_stride + (int64_t)l0 * sj.line_stride;
     const int kind = sj.kind;
     const float b = sj.b;
+    const int rl = threadIdx.x % NR;       // real line of this lane
+    const int pg = threadIdx.x / NR;       // position group
+    const int sidx = 2 * (rl % NL) + rl / NL;  // float offset of (line, component)
+    const bool lane_ok = rl < nreal;
+    float *lsrc = base + (int64_t)rl * sj.line_stride;
 
     // ---- load (padding rule fused) ---------------------------------------
     double acc_in = 0.0;
     if (kind == PASS_X) {
-        const int ny = sj.ny;
-        for (int q = 0; q < 2 * NL; ++q) {
-            float *plane = (q < NL) ? re : im;
-            const int ln = q & (NL - 1);
-            bool rowin = false;
-            if (q < nreal) {
-                const int row = l0 + q;
-                const int y = row % ny, z = row / ny;
-                rowin = y >= sj.box_lo[1] && y < sj.box_hi[1] && z >= sj.box_lo[2] && z < sj.box_hi[2];
+        // positions contiguous: float4 along the line when aligned
+        bool rowin = false;
+        if (lane_ok) {
+            const int row = l0 + rl;
+            const int y = row % sj.ny, z = row / sj.ny;
+            rowin = y >= sj.box_lo[1] && y < sj.box_hi[1] && z >= sj.box_lo[2] && z < sj.box_hi[2];
+        }
+        const int xlo = sj.box_lo[0], xhi = sj.box_hi[0];
+        const bool vec = ((n & 3) == 0) && ((sj.line_stride & 3) == 0) &&
+                         ((reinterpret_cast<uintptr_t>(sj.data) & 15) == 0);
+        if (vec) {
+            const int nc = n >> 2;
+            for (int c0 = pg; c0 < nc; c0 += NPG * U) {
+                float4 r[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int c = c0 + u * NPG;
+                    r[u] = (rowin && c < nc) ? __ldg(reinterpret_cast<const float4 *>(lsrc) + c)
+                                             : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int c = c0 + u * NPG;
+                    if (c < nc) {
+                        const float e[4] = {r[u].x, r[u].y, r[u].z, r[u].w};
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            const int pos = 4 * c + i;
+                            const float v = (rowin && pos >= xlo && pos < xhi) ? e[i] - b : 0.0f;
+                            Sf[pos * 2 * LS + sidx] = v;
+                            acc_in += (double)v;
+                        }
+                    }
+                }
             }
-            const float *src = base + (int64_t)q * sj.line_stride;
-            for (int pos = threadIdx.x; pos < n; pos += NT) {
-                float v = 0.0f;
-                if (rowin && pos >= sj.box_lo[0] && pos < sj.box_hi[0]) v = src[pos] - b;
-                plane[pos * LS + ln] = v;
-                acc_in += (double)v;
+        } else {
+            for (int p0 = pg; p0 < n; p0 += NPG * U) {
+                float r[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int p = p0 + u * NPG;
+                    r[u] = (rowin && p < n) ? __ldg(lsrc + p) : 0.0f;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int p = p0 + u * NPG;
+                    if (p < n) {
+                        const float v = (rowin && p >= xlo && p < xhi) ? r[u] - b : 0.0f;
+                        Sf[p * 2 * LS + sidx] = v;
+                        acc_in += (double)v;
+                    }
+                }
             }
         }
     } else {
         const int64_t ps = sj.pos_stride;
-        for (int idx = threadIdx.x; idx < n * 2 * NL; idx += NT) {
-            const int q = idx & (2 * NL - 1);
-            const int pos = idx >> 5;
-            const float v = (q < nreal) ? base[q * sj.line_stride + pos * ps] : 0.0f;
-            ((q < NL) ? re : im)[pos * LS + (q & (NL - 1))] = v;
+        for (int p0 = pg; p0 < n; p0 += NPG * U) {
+            float r[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int p = p0 + u * NPG;
+                r[u] = (lane_ok && p < n) ? __ldg(lsrc + p * ps) : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int p = p0 + u * NPG;
+                if (p < n) Sf[p * 2 * LS + sidx] = r[u];
+            }
         }
     }
-    for (int i = n * LS + threadIdx.x; i < F * LS; i += NT) {
-        re[i] = 0.0f;
-        im[i] = 0.0f;
-    }
+    for (int i = n * LS + threadIdx.x; i < F * LS; i += NT) S[i] = make_float2(0.f, 0.f);
     __syncthreads();
 
     // ---- forward FFT, spectrum multiply, inverse FFT ---------------------
-    const int line = threadIdx.x & (NL - 1);
+    const int line = threadIdx.x % NL;
     const int tj = threadIdx.x / NL;
-    fft_lines<MAXP, TL, false>(re, im, sj.plan, line, tj, tw);
+    fft_lines<MAXP, TL, NL, false>(S, sj.plan, line, tj, tw);
     for (int i = threadIdx.x; i < F * NL; i += NT) {
-        const int k = i / NL, l = i & (NL - 1);
+        const int k = i / NL, l = i % NL;
         const float g = G[k];
-        re[k * LS + l] *= g;
-        im[k * LS + l] *= g;
+        float2 &x = S[k * LS + l];
+        x.x *= g;
+        x.y *= g;
     }
     __syncthreads();
-    fft_lines<MAXP, TL, true>(re, im, sj.plan, line, tj, tw);
+    fft_lines<MAXP, TL, NL, true>(S, sj.plan, line, tj, tw);
 
     // ---- crop / store (baseline + decay + mass fused into the z pass) ----
     double acc_leak = 0.0, acc_conv = 0.0, acc_out = 0.0;
     for (int i = threadIdx.x; i < (F - n) * NL; i += NT) {
-        const int p = (n + i / NL) * LS + (i & (NL - 1));
-        acc_leak += (double)re[p] + (double)im[p];
+        const float2 x = S[(n + i / NL) * LS + (i % NL)];
+        acc_leak += (double)x.x + (double)x.y;
     }
-    if (kind == PASS_X) {
-        for (int q = 0; q < nreal; ++q) {
-            const float *plane = (q < NL) ? re : im;
-            const int ln = q & (NL - 1);
-            float *dst = base + (int64_t)q * sj.line_stride;
-            for (int pos = threadIdx.x; pos < n; pos += NT) dst[pos] = plane[pos * LS + ln];
-        }
-    } else {
-        const int64_t ps = sj.pos_stride;
-        const bool last = (kind == PASS_Z);
-        const float keep = sj.keep;
-        for (int idx = threadIdx.x; idx < n * 2 * NL; idx += NT) {
-            const int q = idx & (2 * NL - 1);
-            const int pos = idx >> 5;
-            if (q < nreal) {
-                float t = ((q < NL) ? re : im)[pos * LS + (q & (NL - 1))];
+    if (lane_ok) {
+        if (kind == PASS_X) {
+            float *dst = lsrc;
+            const bool vec = ((n & 3) == 0) && ((sj.line_stride & 3) == 0) &&
+                             ((reinterpret_cast<uintptr_t>(sj.data) & 15) == 0);
+            if (vec) {
+                const int nc = n >> 2;
+                for (int c = pg; c < nc; c += NPG) {
+                    float4 o;
+                    o.x = Sf[(4 * c + 0) * 2 * LS + sidx];
+                    o.y = Sf[(4 * c + 1) * 2 * LS + sidx];
+                    o.z = Sf[(4 * c + 2) * 2 * LS + sidx];
+                    o.w = Sf[(4 * c + 3) * 2 * LS + sidx];
+                    reinterpret_cast<float4 *>(dst)[c] = o;
+                }
+            } else {
+                for (int p = pg; p < n; p += NPG) dst[p] = Sf[p * 2 * LS + sidx];
+            }
+        } else {
+            const int64_t ps = sj.pos_stride;
+            const bool last = (kind == PASS_Z);
+            const float keep = sj.keep;
+            for (int p = pg; p < n; p += NPG) {
+                float t = Sf[p * 2 * LS + sidx];
                 if (last) {
                     acc_conv += (double)t;
                     t = keep * (t + b);
                     acc_out += (double)t;
                 }
-                base[q * sj.line_stride + pos * ps] = t;
+                lsrc[p * ps] = t;
             }
         }
     }
@@ -247,21 +309,21 @@ __global__ void __launch_bounds__(256) deposit_kernel(const DepositJob *__restri
 // ---------------------------------------------------------------------------
 // Launch wrappers
 // ---------------------------------------------------------------------------
-template <int TL, int MAXP>
+template <int NL, int TL, int MAXP, int MINB>
 static cudaError_t launch_axis_t(const AxisJob *jobs, int njobs, int tiles, int Fmax, cudaStream_t st)
 {
-    const size_t sm = axis_smem_bytes(Fmax);
+    const size_t sm = axis_smem_bytes(Fmax, NL);
     static thread_local int configured_dev = -1;
     int dev = 0;
     cudaGetDevice(&dev);
     if (configured_dev != dev) {
-        cudaError_t e = cudaFuncSetAttribute(axis_pass_kernel<TL, MAXP>,
+        cudaError_t e = cudaFuncSetAttribute(axis_pass_kernel<NL, TL, MAXP, MINB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)axis_smem_limit());
         if (e != cudaSuccess) return e;
         configured_dev = dev;
     }
-    axis_pass_kernel<TL, MAXP><<<tiles, NL * TL, sm, st>>>(jobs, njobs);
+    axis_pass_kernel<NL, TL, MAXP, MINB><<<tiles, NL * TL, sm, st>>>(jobs, njobs);
     note_launch();
     return cudaGetLastError();
 }
@@ -270,11 +332,10 @@ cudaError_t launch_axis(int variant, const AxisJob *jobs, int njobs, int tiles, 
 {
     if (tiles <= 0) return cudaSuccess;
     switch (variant) {
-    case 0: return launch_axis_t<16, 24>(jobs, njobs, tiles, Fmax, st);
-    case 1: return launch_axis_t<32, 16>(jobs, njobs, tiles, Fmax, st);
-    case 2: return launch_axis_t<32, 24>(jobs, njobs, tiles, Fmax, st);
-    case 3: return launch_axis_t<16, 40>(jobs, njobs, tiles, Fmax, st);
-    case 4: return launch_axis_t<32, 40>(jobs, njobs, tiles, Fmax, st);
+#define VFD_VARIANT_CASE(i, NL, TL, MAXP, MINB) \
+    case i: return launch_axis_t<NL, TL, MAXP, MINB>(jobs, njobs, tiles, Fmax, st);
+        VFD_AXIS_VARIANTS(VFD_VARIANT_CASE)
+#undef VFD_VARIANT_CASE
     default: return cudaErrorInvalidValue;
     }
 }

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "vfd.h"
+#include "vfd_general.h"
 #include "vfd_internal.h"
 
 namespace vfd {
@@ -46,22 +47,28 @@ static bool make_plan(int F, FftPlan *p)
             n /= r;
         }
     }
-    if (n != 1 || F < 2) return false;
+    if (n != 1 || F < 2 || F > 2047) return false;
     p->F = F;
     p->nst = k;
-    for (int i = k; i < MAX_STAGES; ++i) p->radix[i] = 1;
+    int ns = 1;
+    for (int i = 0; i < MAX_STAGES; ++i) {
+        if (i >= k) p->radix[i] = 1;
+        p->ns[i] = ns;
+        p->ns_magic[i] = (int)(((1 << 21) + ns - 1) / ns);
+        ns *= p->radix[i];
+    }
     return true;
 }
 
 static bool variant_fits(int v, const FftPlan &p)
 {
-    const int TL = variant_tl(v), MAXP = variant_maxp(v);
+    const int TL = kAxisVariants[v].tl, MAXP = kAxisVariants[v].maxp;
     for (int s = 0; s < p.nst; ++s) {
         const int R = p.radix[s];
         const int M = p.F / R;
         if ((M + TL - 1) / TL > MAXP / R) return false;
     }
-    return axis_smem_bytes(p.F) <= axis_smem_limit();
+    return axis_smem_bytes(p.F, kAxisVariants[v].nl) <= axis_smem_limit();
 }
 
 static double plan_cost(const FftPlan &p)
@@ -88,13 +95,14 @@ static bool any_variant_fits(const FftPlan &p)
     return false;
 }
 
-static int choose_fft_len(int n, int r)
+static int choose_fft_len(int n, int r, bool even)
 {
     const int lo = n + r;
     int best = -1;
     double best_cost = 0.0;
     for (int F = lo; F <= 2 * lo + 16; ++F) {
         FftPlan p;
+        if (even && (F & 1)) continue;
         if (!make_plan(F, &p) || !any_variant_fits(p)) continue;
         const double c = plan_cost(p);
         if (best < 0 || c < best_cost) {
@@ -105,20 +113,23 @@ static int choose_fft_len(int n, int r)
     return best;
 }
 
-static int pick_variant(const std::vector<FftPlan> &plans)
+static int pick_variant(const std::vector<FftPlan> &plans, int need_nl = 0)
 {
     static int forced = -2;
     if (forced == -2) {
         const char *e = getenv("VFD_AXIS_VARIANT");
         forced = e ? atoi(e) : -1;
     }
-    if (forced >= 0 && forced < kNumAxisVariants) {
+    if (forced >= 0 && forced < kNumAxisVariants && (need_nl == 0 || kAxisVariants[forced].nl == need_nl)) {
         bool ok = true;
         for (const auto &p : plans) ok = ok && variant_fits(forced, p);
         if (ok) return forced;
     }
-    static const int pref[] = {0, 1, 2, 3, 4};
+    // measured on B200 (512x256x384 world, 8 fields): 16-line tiles with 32
+    // threads per line and 2 resident blocks first
+    static const int pref[] = {2, 3, 1, 0, 5, 4};
     for (int v : pref) {
+        if (need_nl && kAxisVariants[v].nl != need_nl) continue;
         bool ok = true;
         for (const auto &p : plans) ok = ok && variant_fits(v, p);
         if (ok) return v;
@@ -192,6 +203,7 @@ struct vfd_world {
     int dep_njobs = 0;
     std::vector<int64_t> src_begin;  // per field begin in concatenated list
     std::vector<int64_t> src_count;
+    uint64_t src_gen = 0;            // bumped whenever the device source lists change
 
     // optional per-launch event timing
     bool profiling = false;
@@ -204,6 +216,15 @@ struct vfd_world {
 
     cudaStream_t s_in = nullptr, s_cmp = nullptr, s_out = nullptr;
     std::vector<cudaEvent_t> ev_in, ev_cmp;
+
+    // general 3D methods (VFD_METHOD_FFT3D / VFD_METHOD_PLAIN)
+    int method = VFD_METHOD_SEPARABLE;
+    int Fxh = 0;
+    int gvar[3] = {0, 0, 0};         // kernel variants of the x rows, y and z columns
+    float2 *d_kspec = nullptr;       // [f][Fz][Fy][Fxh], unscaled K
+    float2 *d_C = nullptr;           // spectrum scratch
+    float *d_P = nullptr;            // full real grid scratch (plain)
+    std::vector<float> k0;           // K(0,0,0) = sum of the window, per field
 
     std::string err;
 };
@@ -239,6 +260,9 @@ static void release(vfd_world *w)
     cudaFree(w->d_src_idx);
     cudaFree(w->d_src_amt);
     cudaFree(w->d_dep);
+    cudaFree(w->d_kspec);
+    cudaFree(w->d_C);
+    cudaFree(w->d_P);
     for (auto &t : w->timed) {
         cudaEventDestroy(t.start);
         cudaEventDestroy(t.stop);
@@ -253,7 +277,16 @@ static void release(vfd_world *w)
 }
 
 // Builds the AxisJob of (field f, axis a).
-static AxisJob make_job(const vfd_world *w, int f, int a, int tile_begin)
+// Tiles of one field for axis a when a launch uses nl lines per tile.
+static int field_tiles(const vfd_world *w, int a, int nl)
+{
+    const int nr = 2 * nl;
+    if (a == PASS_X) return (w->ny * w->nz + nr - 1) / nr;
+    if (a == PASS_Y) return w->nz * ((w->nx + nr - 1) / nr);
+    return w->ny * ((w->nx + nr - 1) / nr);
+}
+
+static AxisJob make_job(const vfd_world *w, int f, int a, int tile_begin, int nl)
 {
     AxisJob j;
     memset(&j, 0, sizeof(j));
@@ -300,7 +333,8 @@ static AxisJob make_job(const vfd_world *w, int f, int a, int tile_begin)
         j.nlines = w->nx;
         j.nouter = w->ny;
     }
-    j.tiles_per_outer = (j.nlines + 2 * NL - 1) / (2 * NL);
+    const int nr = 2 * nl;
+    j.tiles_per_outer = (j.nlines + nr - 1) / nr;
     j.tile_begin = tile_begin;
     return j;
 }
@@ -353,6 +387,12 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
     w->pad_mode = d->pad_mode;
     w->epi = d->epi_boundary;
     w->params.assign(d->fields, d->fields + d->n_fields);
+    w->method = d->method;
+    if (w->method < VFD_METHOD_SEPARABLE || w->method > VFD_METHOD_PLAIN) {
+        delete w;
+        return fail(nullptr, VFD_ERR_INVALID_ARG, "unknown method");
+    }
+    const bool general = w->method != VFD_METHOD_SEPARABLE;
     const int dims[3] = {d->nx, d->ny, d->nz};
     // per-axis radius: the largest over fields (one FFT grid per world)
     int rmax[3] = {0, 0, 0};
@@ -378,12 +418,16 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
                 delete w;
                 return fail(nullptr, VFD_ERR_INVALID_ARG, "fft length shorter than n + radius");
             }
+            if (general && a == 0 && (F & 1)) {
+                delete w;
+                return fail(nullptr, VFD_ERR_INVALID_ARG, "the general 3D methods need an even x FFT length");
+            }
             if (!make_plan(F, &w->plan[a]) || !any_variant_fits(w->plan[a])) {
                 delete w;
                 return fail(nullptr, VFD_ERR_NOT_SUPPORTED, "fft length not 7-smooth or too long");
             }
         } else {
-            F = choose_fft_len(dims[a], rmax[a]);
+            F = choose_fft_len(dims[a], rmax[a], general && a == 0);
             if (F < 0) {
                 delete w;
                 return fail(nullptr, VFD_ERR_NOT_SUPPORTED, "axis too long for the shared-memory FFT");
@@ -394,9 +438,24 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
         w->Fmax = std::max(w->Fmax, F);
         w->variant[a] = pick_variant(std::vector<FftPlan>{w->plan[a]});
     }
-    w->tiles_per_field[0] = (w->ny * w->nz + 2 * NL - 1) / (2 * NL);
-    w->tiles_per_field[1] = w->nz * ((w->nx + 2 * NL - 1) / (2 * NL));
-    w->tiles_per_field[2] = w->ny * ((w->nx + 2 * NL - 1) / (2 * NL));
+    for (int a = 0; a < 3; ++a) {
+        if (w->variant[a] < 0) {
+            delete w;
+            return fail(nullptr, VFD_ERR_NOT_SUPPORTED, "no kernel variant fits the FFT plan");
+        }
+    }
+    for (int a = 0; a < 3; ++a) w->tiles_per_field[a] = field_tiles(w, a, kAxisVariants[w->variant[a]].nl);
+    if (general) {
+        w->Fxh = w->F[0] / 2 + 1;
+        w->gvar[0] = w->variant[0];
+        for (int a = 1; a < 3; ++a) {
+            w->gvar[a] = pick_variant(std::vector<FftPlan>{w->plan[a]}, 16);
+            if (w->gvar[a] < 0) {
+                delete w;
+                return fail(nullptr, VFD_ERR_NOT_SUPPORTED, "no 16-line kernel variant fits the FFT plan");
+            }
+        }
+    }
 
     int prev = 0;
     cudaGetDevice(&prev);
@@ -438,17 +497,34 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
         for (int a = 0; a < 3; ++a) {
             int tb = 0;
             for (int f = 0; f < w->nf; ++f) {
-                jobs.push_back(make_job(w, f, a, tb));
+                jobs.push_back(make_job(w, f, a, tb, kAxisVariants[w->variant[a]].nl));
                 tb += w->tiles_per_field[a];
             }
         }
         for (int a = 0; a < 3; ++a)
-            for (int f = 0; f < w->nf; ++f) jobs.push_back(make_job(w, f, a, 0));
+            for (int f = 0; f < w->nf; ++f) jobs.push_back(make_job(w, f, a, 0, kAxisVariants[w->variant[a]].nl));
         if ((e = cudaMalloc(&w->d_jobs, sizeof(AxisJob) * jobs.size())) != cudaSuccess) return bail(e, "cudaMalloc jobs");
         if ((e = cudaMemcpy(w->d_jobs, jobs.data(), sizeof(AxisJob) * jobs.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
             return bail(e, "cudaMemcpy jobs");
     }
     if ((e = cudaMalloc(&w->d_dep, sizeof(DepositJob) * 2 * w->nf)) != cudaSuccess) return bail(e, "cudaMalloc deposit jobs");
+    if (general) {
+        const int64_t nk = (int64_t)w->Fxh * w->F[1] * w->F[2];
+        if ((e = cudaMalloc(&w->d_kspec, sizeof(float2) * nk * w->nf)) != cudaSuccess) return bail(e, "cudaMalloc spectra");
+        for (int f = 0; f < w->nf; ++f) {
+            const float *sp = w->d_spec + (int64_t)f * 3 * w->Fmax;
+            if ((e = launch_outer_spectrum(w->d_kspec + nk * f, sp, sp + w->Fmax, sp + 2 * w->Fmax, w->F[0], w->F[1],
+                                           w->F[2], 0)) != cudaSuccess)
+                return bail(e, "outer spectrum");
+        }
+        w->k0.assign(w->nf, 1.0f);
+        const int64_t nc = (w->method == VFD_METHOD_PLAIN) ? nk : (int64_t)w->Fxh * w->F[1] * w->nz;
+        if ((e = cudaMalloc(&w->d_C, sizeof(float2) * nc)) != cudaSuccess) return bail(e, "cudaMalloc spectrum scratch");
+        if (w->method == VFD_METHOD_PLAIN) {
+            if ((e = cudaMalloc(&w->d_P, sizeof(float) * (int64_t)w->F[0] * w->F[1] * w->F[2])) != cudaSuccess)
+                return bail(e, "cudaMalloc padded grid");
+        }
+    }
     if ((e = cudaStreamCreateWithFlags(&w->s_in, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
     if ((e = cudaStreamCreateWithFlags(&w->s_cmp, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
     if ((e = cudaStreamCreateWithFlags(&w->s_out, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
@@ -491,6 +567,12 @@ vfd_status vfd_world_device_bytes(const vfd_world *w, size_t *bytes)
     b += sizeof(float) * (size_t)w->nf * 3 * w->Fmax + sizeof(double) * MS_COUNT * w->nf;
     b += sizeof(AxisJob) * 6 * w->nf + sizeof(DepositJob) * 2 * w->nf;
     b += (sizeof(int32_t) + sizeof(float)) * (size_t)w->src_cap;
+    if (w->method != VFD_METHOD_SEPARABLE) {
+        const size_t nk = (size_t)w->Fxh * w->F[1] * w->F[2];
+        b += sizeof(float2) * nk * w->nf;
+        b += sizeof(float2) * ((w->method == VFD_METHOD_PLAIN) ? nk : (size_t)w->Fxh * w->F[1] * w->nz);
+        if (w->method == VFD_METHOD_PLAIN) b += sizeof(float) * (size_t)w->F[0] * w->F[1] * w->F[2];
+    }
     *bytes = b;
     return VFD_OK;
 }
@@ -551,6 +633,103 @@ vfd_status vfd_set_sources(vfd_world *w, int field, const int32_t *idx, const fl
     return VFD_OK;
 }
 
+static void interior_box(const vfd_world *w, int *lo, int *hi)
+{
+    if (w->pad_mode == VFD_PAD_CONSTANT_VF) {
+        lo[0] = 1; hi[0] = std::min(w->epi, w->nx);
+        lo[1] = 1; hi[1] = w->ny - 1;
+        lo[2] = 1; hi[2] = w->nz - 1;
+    } else {
+        lo[0] = 0; hi[0] = w->nx;
+        lo[1] = 0; hi[1] = w->ny;
+        lo[2] = 0; hi[2] = w->nz;
+    }
+}
+
+static GenColPass col_pass(const vfd_world *w, int a, float2 *data, int nouter, int nload, int nstore, int mode)
+{
+    GenColPass c;
+    memset(&c, 0, sizeof(c));
+    c.plan = w->plan[a];
+    c.tw = w->d_tw[a];
+    c.data = data;
+    c.nlines = w->Fxh;
+    c.nouter = nouter;
+    if (a == PASS_Y) {
+        c.outer_stride = (int64_t)w->F[1] * w->Fxh;
+        c.pos_stride = w->Fxh;
+    } else {
+        c.outer_stride = w->Fxh;
+        c.pos_stride = (int64_t)w->F[1] * w->Fxh;
+    }
+    c.nload = nload;
+    c.nstore = nstore;
+    c.mode = mode;
+    c.scale = 1.0f;
+    return c;
+}
+
+vfd_status vfd_set_window(vfd_world *w, int field, const float *window, int kw, int kh, int kd, int cx, int cy,
+                          int cz)
+{
+    if (!w) return VFD_ERR_INVALID_ARG;
+    if (w->method == VFD_METHOD_SEPARABLE)
+        return fail(w, VFD_ERR_NOT_SUPPORTED, "dense windows need VFD_METHOD_FFT3D or VFD_METHOD_PLAIN");
+    if (field < 0 || field >= w->nf || !window || kw < 1 || kh < 1 || kd < 1 || cx < 0 || cx >= kw || cy < 0 ||
+        cy >= kh || cz < 0 || cz >= kd)
+        return fail(w, VFD_ERR_INVALID_ARG, "bad field, window dims or centre");
+    const int Fx = w->F[0], Fy = w->F[1], Fz = w->F[2];
+    // the wrapped window must not alias onto the data: half-widths within F - n
+    if (std::max(cx, kw - 1 - cx) > Fx - w->nx || std::max(cy, kh - 1 - cy) > Fy - w->ny ||
+        std::max(cz, kd - 1 - cz) > Fz - w->nz)
+        return fail(w, VFD_ERR_INVALID_ARG, "window wider than the FFT padding; pass larger fft lengths");
+    DeviceGuard g(w->device);
+    const int64_t nk = (int64_t)w->Fxh * Fy * Fz;
+    const int64_t np = (int64_t)Fx * Fy * Fz;
+    const int64_t nwin = (int64_t)kw * kh * kd;
+    float *P = nullptr, *dw = nullptr;
+    VFD_CUDA(w, cudaMalloc(&P, sizeof(float) * np));
+    cudaError_t e = cudaMalloc(&dw, sizeof(float) * nwin);
+    if (e != cudaSuccess) {
+        cudaFree(P);
+        return fail(w, VFD_ERR_OUT_OF_MEMORY, "cudaMalloc window");
+    }
+    float2 *K = w->d_kspec + nk * field;
+    double wsum = 0.0;
+    for (int64_t i = 0; i < nwin; ++i) wsum += window[i];
+    auto run = [&]() -> cudaError_t {
+        cudaError_t r;
+        if ((r = cudaMemcpy(dw, window, sizeof(float) * nwin, cudaMemcpyHostToDevice)) != cudaSuccess) return r;
+        if ((r = cudaMemset(P, 0, sizeof(float) * np)) != cudaSuccess) return r;
+        if ((r = launch_wrap_window(P, dw, kw, kh, kd, cx, cy, cz, Fx, Fy, Fz, 0)) != cudaSuccess) return r;
+        GenRowPass rp;
+        memset(&rp, 0, sizeof(rp));
+        rp.plan = w->plan[0];
+        rp.tw = w->d_tw[0];
+        rp.nrows = Fy * Fz;
+        rp.rows_per_plane = Fy;
+        rp.r_s1 = Fx;
+        rp.r_s2 = (int64_t)Fx * Fy;
+        rp.c_s1 = w->Fxh;
+        rp.c_s2 = (int64_t)w->Fxh * Fy;
+        rp.nload = Fx;
+        rp.rsrc = P;
+        rp.cdst = K;
+        if ((r = launch_gen_rows(w->gvar[0], rp, false, 0)) != cudaSuccess) return r;
+        if ((r = launch_gen_cols(w->gvar[1], col_pass(w, PASS_Y, K, Fz, Fy, Fy, GEN_FORWARD), 0)) != cudaSuccess)
+            return r;
+        if ((r = launch_gen_cols(w->gvar[2], col_pass(w, PASS_Z, K, Fy, Fz, Fz, GEN_FORWARD), 0)) != cudaSuccess)
+            return r;
+        return cudaDeviceSynchronize();
+    };
+    e = run();
+    cudaFree(P);
+    cudaFree(dw);
+    if (e != cudaSuccess) return fail(w, VFD_ERR_CUDA, std::string("window spectrum: ") + cudaGetErrorString(e));
+    w->k0[field] = (float)wsum;
+    return VFD_OK;
+}
+
 // Uploads the concatenated source list and deposit jobs when they changed.
 static vfd_status sync_sources(vfd_world *w)
 {
@@ -606,6 +785,7 @@ static vfd_status sync_sources(vfd_world *w)
     VFD_CUDA(w, cudaMemcpy(w->d_dep, jobs.data(), sizeof(DepositJob) * jobs.size(), cudaMemcpyHostToDevice));
     w->src_total = total;
     w->src_dirty = false;
+    w->src_gen++;
     return VFD_OK;
 }
 
@@ -644,9 +824,128 @@ struct LaunchTimer {
     }
 };
 
+// One substep of field f with the general 3D transform.
+static vfd_status enqueue_general_substep(vfd_world *w, int f, cudaStream_t st)
+{
+    const int Fx = w->F[0], Fy = w->F[1], Fz = w->F[2];
+    const int64_t nk = (int64_t)w->Fxh * Fy * Fz;
+    float *u = w->d_fields + (int64_t)f * w->V;
+    double *mass = w->d_mass + (int64_t)f * MS_COUNT;
+    const float2 *K = w->d_kspec + nk * f;
+    const float invN = (float)(1.0 / ((double)Fx * Fy * Fz));
+    const float b = w->pad_mode == VFD_PAD_CONSTANT_VF ? w->params[f].baseline : 0.0f;
+    const float keep = (float)(1.0 - w->params[f].decay_rate);
+    int lo[3], hi[3];
+    interior_box(w, lo, hi);
+    GenRowPass r;
+    memset(&r, 0, sizeof(r));
+    r.plan = w->plan[0];
+    r.tw = w->d_tw[0];
+    r.c_s1 = w->Fxh;
+    r.c_s2 = (int64_t)w->Fxh * Fy;
+    if (w->method == VFD_METHOD_FFT3D) {
+        // pruned + fused: rows of the data only; C holds z < nz
+        r.nrows = w->ny * w->nz;
+        r.rows_per_plane = w->ny;
+        r.r_s1 = w->nx;
+        r.r_s2 = (int64_t)w->nx * w->ny;
+        r.nload = w->nx;
+        r.nstore = w->nx;
+        r.rsrc = u;
+        r.rdst = u;
+        r.cdst = w->d_C;
+        r.csrc = w->d_C;
+        r.fuse_pad = 1;
+        for (int i = 0; i < 3; ++i) {
+            r.box_lo[i] = lo[i];
+            r.box_hi[i] = hi[i];
+        }
+        r.b = b;
+        r.mass_in = mass + MS_INPUT;
+        {
+            LaunchTimer lt(w, 0, st);
+            VFD_CUDA(w, launch_gen_rows(w->gvar[0], r, false, st));
+            lt.done();
+        }
+        {
+            LaunchTimer lt(w, 1, st);
+            VFD_CUDA(w, launch_gen_cols(w->gvar[1], col_pass(w, PASS_Y, w->d_C, w->nz, w->ny, Fy, GEN_FORWARD), st));
+            lt.done();
+        }
+        {
+            GenColPass c = col_pass(w, PASS_Z, w->d_C, Fy, w->nz, w->nz, GEN_FWD_MUL_INV);
+            c.kspec = K;
+            c.k_s_outer = w->Fxh;
+            c.k_s_pos = (int64_t)w->Fxh * Fy;
+            c.scale = invN;
+            LaunchTimer lt(w, 2, st);
+            VFD_CUDA(w, launch_gen_cols(w->gvar[2], c, st));
+            lt.done();
+        }
+        {
+            LaunchTimer lt(w, 1, st);
+            VFD_CUDA(w, launch_gen_cols(w->gvar[1], col_pass(w, PASS_Y, w->d_C, w->nz, Fy, w->ny, GEN_INVERSE), st));
+            lt.done();
+        }
+        r.fuse_pad = 0;
+        r.fuse_crop = 1;
+        r.keep = keep;
+        r.k0 = w->k0[f];
+        r.mass_in = nullptr;
+        r.mass_leak = mass + MS_LEAK_X;
+        r.mass_conv = mass + MS_CONV;
+        r.mass_out = mass + MS_OUT;
+        LaunchTimer lt(w, 0, st);
+        VFD_CUDA(w, launch_gen_rows(w->gvar[0], r, true, st));
+        lt.done();
+        return VFD_OK;
+    }
+    // plain: unfused kernels on the full grid, the reference's order
+    VFD_CUDA(w, launch_pad(w->d_P, u, w->nx, w->ny, w->nz, Fx, Fy, Fz, lo, hi, b, st));
+    VFD_CUDA(w, launch_sum(w->d_P, (int64_t)Fx * Fy * Fz, mass + MS_INPUT, st));
+    r.nrows = Fy * Fz;
+    r.rows_per_plane = Fy;
+    r.r_s1 = Fx;
+    r.r_s2 = (int64_t)Fx * Fy;
+    r.nload = Fx;
+    r.nstore = Fx;
+    r.rsrc = w->d_P;
+    r.rdst = w->d_P;
+    r.cdst = w->d_C;
+    r.csrc = w->d_C;
+    VFD_CUDA(w, launch_gen_rows(w->gvar[0], r, false, st));
+    VFD_CUDA(w, launch_gen_cols(w->gvar[1], col_pass(w, PASS_Y, w->d_C, Fz, Fy, Fy, GEN_FORWARD), st));
+    VFD_CUDA(w, launch_gen_cols(w->gvar[2], col_pass(w, PASS_Z, w->d_C, Fy, Fz, Fz, GEN_FORWARD), st));
+    VFD_CUDA(w, launch_modulate(w->d_C, K, nk, invN, st));
+    VFD_CUDA(w, launch_gen_cols(w->gvar[2], col_pass(w, PASS_Z, w->d_C, Fy, Fz, Fz, GEN_INVERSE), st));
+    VFD_CUDA(w, launch_gen_cols(w->gvar[1], col_pass(w, PASS_Y, w->d_C, Fz, Fy, Fy, GEN_INVERSE), st));
+    VFD_CUDA(w, launch_gen_rows(w->gvar[0], r, true, st));
+    VFD_CUDA(w, launch_sum(w->d_P, (int64_t)Fx * Fy * Fz, mass + MS_LEAK_X, st));  // full-grid sum, see read_mass
+    VFD_CUDA(w, launch_crop(u, w->d_P, w->nx, w->ny, w->nz, Fx, Fy, keep, mass + MS_CONV, mass + MS_OUT, st));
+    return VFD_OK;
+}
+
 // Enqueues n_substeps of one field (field >= 0) or of all fields (field < 0).
 static vfd_status enqueue_tick(vfd_world *w, int field, int n_substeps, cudaStream_t st)
 {
+    if (w->method != VFD_METHOD_SEPARABLE) {
+        const int f0 = field < 0 ? 0 : field, f1 = field < 0 ? w->nf : field + 1;
+        for (int s = 0; s < n_substeps; ++s)
+            for (int f = f0; f < f1; ++f) {
+                VFD_CUDA(w, cudaMemsetAsync(w->d_mass + (int64_t)f * MS_COUNT, 0, sizeof(double) * MS_COUNT, st));
+                vfd_status r = enqueue_general_substep(w, f, st);
+                if (r != VFD_OK) return r;
+            }
+        if (field < 0) {
+            if (w->dep_njobs > 0)
+                VFD_CUDA(w, launch_deposit(w->d_dep, w->dep_njobs, w->d_src_idx, w->d_src_amt, w->src_total,
+                                           w->d_err, st));
+        } else if (w->src_count[field] > 0) {
+            VFD_CUDA(w, launch_deposit(w->d_dep + w->nf + field, 1, w->d_src_idx + w->src_begin[field],
+                                       w->d_src_amt + w->src_begin[field], w->src_count[field], w->d_err, st));
+        }
+        return VFD_OK;
+    }
     const int nj = field < 0 ? w->nf : 1;
     for (int s = 0; s < n_substeps; ++s) {
         if (field < 0)
@@ -702,6 +1001,16 @@ vfd_status vfd_read_mass(vfd_world *w, vfd_mass *out, void *stream)
         out[f].leaked[0] = m[MS_LEAK_X];
         out[f].leaked[1] = m[MS_LEAK_Y];
         out[f].leaked[2] = m[MS_LEAK_Z];
+        if (w->method == VFD_METHOD_PLAIN) {
+            // MS_LEAK_X holds the full-grid sum of the inverse transform
+            out[f].leaked[0] = m[MS_LEAK_X] - m[MS_CONV];
+            out[f].leaked[1] = out[f].leaked[2] = 0.0;
+        } else if (w->method == VFD_METHOD_FFT3D) {
+            // pruned transform: the y/z spill is not materialised; report the
+            // total beyond the crop implied by the kernel sum K0
+            out[f].leaked[0] = m[MS_INPUT] * w->k0[f] - m[MS_CONV];
+            out[f].leaked[1] = out[f].leaked[2] = 0.0;
+        }
         out[f].conv_sum = m[MS_CONV];
         out[f].sources = m[MS_SOURCES];
         out[f].total = m[MS_OUT] + m[MS_SOURCES];
@@ -767,6 +1076,188 @@ vfd_status vfd_diffuse_host(vfd_world *w, const float *const *host_in, float *co
     if (herr) return fail(w, VFD_ERR_DEVICE_FAULT, "a kernel rejected an out-of-range index");
     return VFD_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Batched ensembles: every field of every world goes through one launch per
+// axis pass per substep; the whole tick is captured once into a CUDA graph
+// and replayed (re-captured when the substep count or any world's source
+// lists change).
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct vfd_batch {
+    int device = 0;
+    std::vector<vfd_world *> worlds;
+    int variant[3] = {0, 0, 0};
+    int tiles[3] = {0, 0, 0};
+    int Fmax[3] = {0, 0, 0};
+    int njobs = 0;
+    AxisJob *d_jobs = nullptr;  // [3][njobs]
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int graph_substeps = -1;
+    uint64_t graph_launches = 0;
+    std::vector<uint64_t> gens;
+    std::string err;
+};
+
+static vfd_status bfail(vfd_batch *b, vfd_status s, const std::string &msg)
+{
+    if (b) b->err = msg;
+    else g_thread_error = msg;
+    return s;
+}
+
+#define VFD_BCUDA(b, call)                                                                  \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return bfail((b), e_ == cudaErrorMemoryAllocation ? VFD_ERR_OUT_OF_MEMORY        \
+                                                               : VFD_ERR_CUDA,                \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));               \
+    } while (0)
+
+static void batch_release(vfd_batch *b)
+{
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(b->device);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    cudaFree(b->d_jobs);
+    if (b->ev_in) cudaEventDestroy(b->ev_in);
+    if (b->ev_out) cudaEventDestroy(b->ev_out);
+    if (b->st) cudaStreamDestroy(b->st);
+    cudaSetDevice(prev);
+}
+
+extern "C" {
+
+vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **out)
+{
+    if (!out) return bfail(nullptr, VFD_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    if (!worlds || n_worlds < 1) return bfail(nullptr, VFD_ERR_INVALID_ARG, "no worlds");
+    for (int i = 0; i < n_worlds; ++i) {
+        if (!worlds[i]) return bfail(nullptr, VFD_ERR_INVALID_ARG, "NULL world");
+        if (worlds[i]->device != worlds[0]->device)
+            return bfail(nullptr, VFD_ERR_INVALID_ARG, "worlds of a batch must share one device");
+        if (worlds[i]->method != VFD_METHOD_SEPARABLE)
+            return bfail(nullptr, VFD_ERR_NOT_SUPPORTED, "batches take VFD_METHOD_SEPARABLE worlds");
+    }
+    vfd_batch *b = new vfd_batch();
+    b->device = worlds[0]->device;
+    b->worlds.assign(worlds, worlds + n_worlds);
+    for (int a = 0; a < 3; ++a) {
+        std::vector<FftPlan> plans;
+        for (auto *w : b->worlds) {
+            plans.push_back(w->plan[a]);
+            b->Fmax[a] = std::max(b->Fmax[a], w->F[a]);
+        }
+        b->variant[a] = pick_variant(plans);
+        if (b->variant[a] < 0) {
+            delete b;
+            return bfail(nullptr, VFD_ERR_NOT_SUPPORTED, "no kernel variant fits every world's FFT plan");
+        }
+    }
+    std::vector<AxisJob> jobs;
+    for (int a = 0; a < 3; ++a) {
+        const int nl = kAxisVariants[b->variant[a]].nl;
+        int tb = 0;
+        for (auto *w : b->worlds)
+            for (int f = 0; f < w->nf; ++f) {
+                jobs.push_back(make_job(w, f, a, tb, nl));
+                tb += field_tiles(w, a, nl);
+            }
+        b->tiles[a] = tb;
+    }
+    b->njobs = (int)jobs.size() / 3;
+    DeviceGuard g(b->device);
+    cudaError_t e;
+    if ((e = cudaMalloc(&b->d_jobs, sizeof(AxisJob) * jobs.size())) != cudaSuccess ||
+        (e = cudaMemcpy(b->d_jobs, jobs.data(), sizeof(AxisJob) * jobs.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming)) != cudaSuccess) {
+        std::string msg = std::string("batch setup: ") + cudaGetErrorString(e);
+        batch_release(b);
+        delete b;
+        return bfail(nullptr, e == cudaErrorMemoryAllocation ? VFD_ERR_OUT_OF_MEMORY : VFD_ERR_CUDA, msg);
+    }
+    b->gens.assign(n_worlds, ~0ull);
+    *out = b;
+    return VFD_OK;
+}
+
+vfd_status vfd_batch_destroy(vfd_batch *b)
+{
+    if (!b) return VFD_ERR_INVALID_ARG;
+    batch_release(b);
+    delete b;
+    return VFD_OK;
+}
+
+static vfd_status batch_enqueue(vfd_batch *b, int n_substeps)
+{
+    for (int s = 0; s < n_substeps; ++s) {
+        for (auto *w : b->worlds)
+            VFD_BCUDA(b, cudaMemsetAsync(w->d_mass, 0, sizeof(double) * MS_COUNT * w->nf, b->st));
+        for (int a = 0; a < 3; ++a)
+            VFD_BCUDA(b, launch_axis(b->variant[a], b->d_jobs + a * b->njobs, b->njobs, b->tiles[a],
+                                     b->Fmax[a], b->st));
+    }
+    for (auto *w : b->worlds)
+        if (w->dep_njobs > 0)
+            VFD_BCUDA(b, launch_deposit(w->d_dep, w->dep_njobs, w->d_src_idx, w->d_src_amt, w->src_total,
+                                        w->d_err, b->st));
+    return VFD_OK;
+}
+
+vfd_status vfd_batch_tick(vfd_batch *b, int n_substeps, void *stream)
+{
+    if (!b) return VFD_ERR_INVALID_ARG;
+    if (n_substeps < 1) return bfail(b, VFD_ERR_INVALID_ARG, "n_substeps must be >= 1");
+    DeviceGuard g(b->device);
+    bool stale = (b->exec == nullptr) || (b->graph_substeps != n_substeps);
+    for (size_t i = 0; i < b->worlds.size(); ++i) {
+        vfd_status st = sync_sources(b->worlds[i]);
+        if (st != VFD_OK) return bfail(b, st, b->worlds[i]->err);
+        if (b->gens[i] != b->worlds[i]->src_gen) stale = true;
+    }
+    VFD_BCUDA(b, cudaEventRecord(b->ev_in, (cudaStream_t)stream));
+    VFD_BCUDA(b, cudaStreamWaitEvent(b->st, b->ev_in, 0));
+    if (stale) {
+        if (b->exec) cudaGraphExecDestroy(b->exec);
+        if (b->graph) cudaGraphDestroy(b->graph);
+        b->exec = nullptr;
+        b->graph = nullptr;
+        const uint64_t before = g_launches.load();
+        VFD_BCUDA(b, cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+        vfd_status st = batch_enqueue(b, n_substeps);
+        cudaGraph_t graph = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(b->st, &graph);
+        if (st != VFD_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (ce != cudaSuccess) return bfail(b, VFD_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
+        b->graph = graph;
+        b->graph_launches = g_launches.load() - before;
+        g_launches.fetch_sub(b->graph_launches);  // captured, not executed
+        VFD_BCUDA(b, cudaGraphInstantiate(&b->exec, b->graph, 0));
+        b->graph_substeps = n_substeps;
+        for (size_t i = 0; i < b->worlds.size(); ++i) b->gens[i] = b->worlds[i]->src_gen;
+    }
+    VFD_BCUDA(b, cudaGraphLaunch(b->exec, b->st));
+    g_launches.fetch_add(b->graph_launches);
+    VFD_BCUDA(b, cudaEventRecord(b->ev_out, b->st));
+    VFD_BCUDA(b, cudaStreamWaitEvent((cudaStream_t)stream, b->ev_out, 0));
+    return VFD_OK;
+}
+
+const char *vfd_batch_last_error(const vfd_batch *b) { return b ? b->err.c_str() : g_thread_error.c_str(); }
 
 // ---------------------------------------------------------------------------
 // Synthetic inputs: counter-based splitmix64 (Steele, Lea, Flood 2014

@@ -21,6 +21,10 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libvfd.so")
 PAD_ZERO = 0
 PAD_CONSTANT_VF = 1
 
+METHOD_SEPARABLE = 0
+METHOD_FFT3D = 1
+METHOD_PLAIN = 2
+
 STATUS = {
     0: "VFD_OK", 1: "VFD_ERR_INVALID_ARG", 2: "VFD_ERR_OUT_OF_MEMORY",
     3: "VFD_ERR_BUDGET", 4: "VFD_ERR_CUDA", 5: "VFD_ERR_TIMEOUT",
@@ -35,6 +39,8 @@ EXPORTED = [
     "vfd_diffuse_host", "vfd_status_string", "vfd_last_error",
     "vfd_kernel_launch_count", "vfd_synth_field", "vfd_synth_sources",
     "vfd_world_set_profiling", "vfd_read_profile",
+    "vfd_batch_create", "vfd_batch_tick", "vfd_batch_destroy", "vfd_batch_last_error",
+    "vfd_set_window",
 ]
 
 
@@ -53,7 +59,7 @@ class WorldDesc(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("n_fields", C.c_int), ("fields", C.POINTER(FieldParams)),
                 ("pad_mode", C.c_int), ("epi_boundary", C.c_int),
-                ("fft", C.c_int * 3)]
+                ("fft", C.c_int * 3), ("method", C.c_int)]
 
 
 class Mass(C.Structure):
@@ -86,6 +92,12 @@ def load(path=LIB_PATH):
     lib.vfd_diffuse_host.argtypes = [P, C.POINTER(P), C.POINTER(P), C.c_int]
     lib.vfd_world_set_profiling.argtypes = [P, C.c_int]
     lib.vfd_read_profile.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    lib.vfd_set_window.argtypes = [P, C.c_int, P] + [C.c_int] * 6
+    lib.vfd_batch_create.argtypes = [C.POINTER(P), C.c_int, C.POINTER(P)]
+    lib.vfd_batch_tick.argtypes = [P, C.c_int, P]
+    lib.vfd_batch_destroy.argtypes = [P]
+    lib.vfd_batch_last_error.argtypes = [P]
+    lib.vfd_batch_last_error.restype = C.c_char_p
     lib.vfd_status_string.argtypes = [C.c_int]
     lib.vfd_status_string.restype = C.c_char_p
     lib.vfd_last_error.argtypes = [P]
@@ -96,7 +108,8 @@ def load(path=LIB_PATH):
     lib.vfd_synth_sources.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int64, C.c_int64,
                                       C.c_double, C.c_double, P, P]
     for name in EXPORTED:
-        if name not in ("vfd_status_string", "vfd_last_error", "vfd_kernel_launch_count"):
+        if name not in ("vfd_status_string", "vfd_last_error", "vfd_kernel_launch_count",
+                        "vfd_batch_last_error"):
             getattr(lib, name).restype = C.c_int
     return lib
 
@@ -153,7 +166,7 @@ class World:
     """One world of `n_fields` fields on an nx*ny*nz grid (x fastest)."""
 
     def __init__(self, nx, ny, nz, params, pad_mode=PAD_ZERO, epi_boundary=0,
-                 fft=(0, 0, 0), device=0):
+                 fft=(0, 0, 0), device=0, method=METHOD_SEPARABLE):
         self.nx, self.ny, self.nz = nx, ny, nz
         self.nf = len(params)
         self._params = (FieldParams * self.nf)(*params)
@@ -163,6 +176,7 @@ class World:
         d.pad_mode, d.epi_boundary = pad_mode, epi_boundary
         for a in range(3):
             d.fft[a] = int(fft[a])
+        d.method = int(method)
         h = C.c_void_p()
         _check(lib().vfd_world_create(C.byref(d), device, C.byref(h)))
         self._h = h
@@ -226,6 +240,13 @@ class World:
         assert i.size == a.size
         _check(lib().vfd_set_sources(self._h, field, _ptr(i), _ptr(a), i.size), self._h)
 
+    def set_window(self, field, window, centre=None):
+        """Dense real window (kd, kh, kw) as this field's kernel; centre (cz, cy, cx)."""
+        w = np.ascontiguousarray(window, dtype=np.float32)
+        kd, kh, kw = w.shape
+        cz, cy, cx = centre if centre is not None else (kd // 2, kh // 2, kw // 2)
+        _check(lib().vfd_set_window(self._h, field, _ptr(w), kw, kh, kd, cx, cy, cz), self._h)
+
     def tick(self, n_substeps=1, stream=None):
         _check(lib().vfd_tick(self._h, n_substeps, stream), self._h)
 
@@ -248,6 +269,47 @@ class World:
         ins = (C.c_void_p * self.nf)(*[a.ctypes.data for a in host_in])
         outs = (C.c_void_p * self.nf)(*[a.ctypes.data for a in host_out])
         _check(lib().vfd_diffuse_host(self._h, ins, outs, n_substeps), self._h)
+
+
+class Batch:
+    """Many worlds ticked together: one launch per axis pass per substep for
+    all their fields, the tick captured in a CUDA graph (vfd_batch_*)."""
+
+    def __init__(self, worlds):
+        self.worlds = list(worlds)
+        arr = (C.c_void_p * len(self.worlds))(*[w.handle.value for w in self.worlds])
+        h = C.c_void_p()
+        _check(lib().vfd_batch_create(arr, len(self.worlds), C.byref(h)))
+        self._h = h
+
+    def set_window(self, field, window, centre=None):
+        """Dense real window (kd, kh, kw) as this field's kernel; centre (cz, cy, cx)."""
+        w = np.ascontiguousarray(window, dtype=np.float32)
+        kd, kh, kw = w.shape
+        cz, cy, cx = centre if centre is not None else (kd // 2, kh // 2, kw // 2)
+        _check(lib().vfd_set_window(self._h, field, _ptr(w), kw, kh, kd, cx, cy, cz), self._h)
+
+    def tick(self, n_substeps=1, stream=None):
+        st = lib().vfd_batch_tick(self._h, n_substeps, stream)
+        if st != 0:
+            raise VfdError(st, lib().vfd_batch_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().vfd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def launch_count():
