@@ -220,3 +220,17 @@ def test_cfg1_full_size_one_field_against_oracle(gpu):
     e = rel_l2(outs[0], ref)
     assert e <= REL_L2, e
     check_mass(outs[0], mass[0], 1 - c["decay"][f], 0.0, nx * ny * nz)
+
+
+@pytest.mark.parametrize("sigma", [(6.0, 1.0, 5.5), 6.2])
+def test_wide_kernel_uses_full_line_path(gpu, sigma):
+    """Radius above the overlap-save limit (16) on some axes: those passes run
+    the full-line shared-memory FFT; results still match the oracle."""
+    grid = (80, 50, 44)
+    nx, ny, nz = grid
+    u = vfd.synth_field(8, 0, 0, (nz, ny, nx))
+    idx, amt = vfd.synth_sources(8, 0, 0, 50, nx * ny * nz)
+    outs, mass, _ = run_world(grid, [sigma], [0.03], [(u, idx, amt)], substeps=2)
+    ref = oracle.tick(u, sigma, 0.03, 2, idx, amt)
+    assert rel_l2(outs[0], ref) <= REL_L2
+    check_mass(outs[0], mass[0], 0.97, 0.0, nx * ny * nz)

@@ -21,6 +21,7 @@
 #include "vfd.h"
 #include "vfd_general.h"
 #include "vfd_internal.h"
+#include "vfd_os.h"
 
 namespace vfd {
 
@@ -183,6 +184,11 @@ struct vfd_world {
     FftPlan plan[3];
     int variant[3] = {0, 0, 0};
     int tiles_per_field[3] = {0, 0, 0};
+    // overlap-save passes (kernel radius <= OS_RMAX): per axis
+    bool use_os[3] = {false, false, false};
+    int rmin[3] = {0, 0, 0};
+    OsJob *d_osjobs = nullptr;             // [pass][nf] all-field, then [pass][nf] single-field
+    std::vector<int> os_tiles[3];          // per field
 
     float *d_fields = nullptr;
     float2 *d_tw[3] = {nullptr, nullptr, nullptr};
@@ -256,6 +262,7 @@ static void release(vfd_world *w)
     cudaFree(w->d_spec);
     cudaFree(w->d_mass);
     cudaFree(w->d_jobs);
+    cudaFree(w->d_osjobs);
     cudaFree(w->d_err);
     cudaFree(w->d_src_idx);
     cudaFree(w->d_src_amt);
@@ -338,6 +345,52 @@ static AxisJob make_job(const vfd_world *w, int f, int a, int tile_begin, int nl
     j.tile_begin = tile_begin;
     return j;
 }
+
+static bool os_enabled()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("VFD_OS");
+        on = (e && e[0] == '0') ? 0 : 1;
+    }
+    return on == 1;
+}
+
+static OsJob make_os_job(const vfd_world *w, int f, int a, int tile_begin)
+{
+    const AxisJob aj = make_job(w, f, a, 0, 16);
+    OsJob j;
+    memset(&j, 0, sizeof(j));
+    j.data = aj.data;
+    j.mass = aj.mass;
+    j.line_stride = aj.line_stride;
+    j.outer_stride = aj.outer_stride;
+    j.pos_stride = aj.pos_stride;
+    j.n = aj.n;
+    j.nlines = aj.nlines;
+    j.nouter = aj.nouter;
+    j.r = w->params[f].radius[a];
+    j.L = OS_N - 2 * j.r;
+    j.C = OS_M * j.L;
+    j.nchunks = (j.n + 2 * j.r + j.C - 1) / j.C;
+    j.tiles_per_outer = ((j.nlines + 31) / 32) * j.nchunks;
+    j.tile_begin = tile_begin;
+    j.kind = a;
+    j.b = aj.b;
+    j.keep = aj.keep;
+    j.nx = aj.nx;
+    j.ny = aj.ny;
+    for (int i = 0; i < 3; ++i) {
+        j.box_lo[i] = aj.box_lo[i];
+        j.box_hi[i] = aj.box_hi[i];
+    }
+    std::vector<float> h;
+    gauss_spectrum(w->params[f].sigma[a], j.r, OS_N, h);
+    for (int k = 0; k < OS_N; ++k) j.H[k] = h[k];
+    return j;
+}
+
+static int os_field_tiles(const OsJob &j) { return j.nouter * j.tiles_per_outer; }
 
 extern "C" {
 
@@ -445,6 +498,14 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
         }
     }
     for (int a = 0; a < 3; ++a) w->tiles_per_field[a] = field_tiles(w, a, kAxisVariants[w->variant[a]].nl);
+    if (!general && os_enabled()) {
+        for (int a = 0; a < 3; ++a) {
+            int rmn = 1 << 30;
+            for (int f = 0; f < w->nf; ++f) rmn = std::min(rmn, w->params[f].radius[a]);
+            w->use_os[a] = rmax[a] <= OS_RMAX;
+            w->rmin[a] = rmn;
+        }
+    }
     if (general) {
         w->Fxh = w->F[0] / 2 + 1;
         w->gvar[0] = w->variant[0];
@@ -506,6 +567,23 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
         if ((e = cudaMalloc(&w->d_jobs, sizeof(AxisJob) * jobs.size())) != cudaSuccess) return bail(e, "cudaMalloc jobs");
         if ((e = cudaMemcpy(w->d_jobs, jobs.data(), sizeof(AxisJob) * jobs.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
             return bail(e, "cudaMemcpy jobs");
+    }
+    if (w->use_os[0] || w->use_os[1] || w->use_os[2]) {
+        std::vector<OsJob> oj;
+        for (int a = 0; a < 3; ++a) {
+            int tb = 0;
+            w->os_tiles[a].assign(w->nf, 0);
+            for (int f = 0; f < w->nf; ++f) {
+                oj.push_back(make_os_job(w, f, a, tb));
+                w->os_tiles[a][f] = os_field_tiles(oj.back());
+                tb += w->os_tiles[a][f];
+            }
+        }
+        for (int a = 0; a < 3; ++a)
+            for (int f = 0; f < w->nf; ++f) oj.push_back(make_os_job(w, f, a, 0));
+        if ((e = cudaMalloc(&w->d_osjobs, sizeof(OsJob) * oj.size())) != cudaSuccess) return bail(e, "cudaMalloc os jobs");
+        if ((e = cudaMemcpy(w->d_osjobs, oj.data(), sizeof(OsJob) * oj.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail(e, "cudaMemcpy os jobs");
     }
     if ((e = cudaMalloc(&w->d_dep, sizeof(DepositJob) * 2 * w->nf)) != cudaSuccess) return bail(e, "cudaMalloc deposit jobs");
     if (general) {
@@ -953,10 +1031,21 @@ static vfd_status enqueue_tick(vfd_world *w, int field, int n_substeps, cudaStre
         else
             VFD_CUDA(w, cudaMemsetAsync(w->d_mass + (int64_t)field * MS_COUNT, 0, sizeof(double) * MS_COUNT, st));
         for (int a = 0; a < 3; ++a) {
-            const AxisJob *jobs = field < 0 ? w->d_jobs + a * w->nf : w->d_jobs + 3 * w->nf + a * w->nf + field;
-            const int tiles = w->tiles_per_field[a] * nj;
             LaunchTimer lt(w, a, st);
-            VFD_CUDA(w, launch_axis(w->variant[a], jobs, nj, tiles, w->F[a], st));
+            if (w->use_os[a]) {
+                const OsJob *jobs =
+                    field < 0 ? w->d_osjobs + a * w->nf : w->d_osjobs + 3 * w->nf + a * w->nf + field;
+                int tiles = 0;
+                if (field < 0)
+                    for (int f = 0; f < w->nf; ++f) tiles += w->os_tiles[a][f];
+                else
+                    tiles = w->os_tiles[a][field];
+                VFD_CUDA(w, launch_os(jobs, nj, tiles, w->rmin[a], st));
+            } else {
+                const AxisJob *jobs = field < 0 ? w->d_jobs + a * w->nf : w->d_jobs + 3 * w->nf + a * w->nf + field;
+                const int tiles = w->tiles_per_field[a] * nj;
+                VFD_CUDA(w, launch_axis(w->variant[a], jobs, nj, tiles, w->F[a], st));
+            }
             lt.done();
         }
     }
@@ -1093,6 +1182,10 @@ struct vfd_batch {
     int Fmax[3] = {0, 0, 0};
     int njobs = 0;
     AxisJob *d_jobs = nullptr;  // [3][njobs]
+    bool use_os[3] = {false, false, false};
+    int rmin[3] = {0, 0, 0};
+    OsJob *d_osjobs = nullptr;  // [3][njobs]
+    int os_tiles[3] = {0, 0, 0};
     cudaStream_t st = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     cudaGraph_t graph = nullptr;
@@ -1127,6 +1220,7 @@ static void batch_release(vfd_batch *b)
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     cudaFree(b->d_jobs);
+    cudaFree(b->d_osjobs);
     if (b->ev_in) cudaEventDestroy(b->ev_in);
     if (b->ev_out) cudaEventDestroy(b->ev_out);
     if (b->st) cudaStreamDestroy(b->st);
@@ -1174,7 +1268,39 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
         b->tiles[a] = tb;
     }
     b->njobs = (int)jobs.size() / 3;
+    std::vector<OsJob> oj;
+    for (int a = 0; a < 3; ++a) {
+        bool all = true;
+        int rmn = 1 << 30;
+        for (auto *w : b->worlds) {
+            all = all && w->use_os[a];
+            for (int f = 0; f < w->nf; ++f) rmn = std::min(rmn, w->params[f].radius[a]);
+        }
+        b->use_os[a] = all;
+        b->rmin[a] = rmn;
+    }
+    if (b->use_os[0] || b->use_os[1] || b->use_os[2]) {
+        for (int a = 0; a < 3; ++a) {
+            int tb = 0;
+            for (auto *w : b->worlds)
+                for (int f = 0; f < w->nf; ++f) {
+                    oj.push_back(make_os_job(w, f, a, tb));
+                    tb += os_field_tiles(oj.back());
+                }
+            b->os_tiles[a] = tb;
+        }
+    }
     DeviceGuard g(b->device);
+    if (!oj.empty()) {
+        cudaError_t e2;
+        if ((e2 = cudaMalloc(&b->d_osjobs, sizeof(OsJob) * oj.size())) != cudaSuccess ||
+            (e2 = cudaMemcpy(b->d_osjobs, oj.data(), sizeof(OsJob) * oj.size(), cudaMemcpyHostToDevice)) != cudaSuccess) {
+            std::string msg = std::string("batch os jobs: ") + cudaGetErrorString(e2);
+            batch_release(b);
+            delete b;
+            return bfail(nullptr, VFD_ERR_CUDA, msg);
+        }
+    }
     cudaError_t e;
     if ((e = cudaMalloc(&b->d_jobs, sizeof(AxisJob) * jobs.size())) != cudaSuccess ||
         (e = cudaMemcpy(b->d_jobs, jobs.data(), sizeof(AxisJob) * jobs.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
@@ -1204,9 +1330,13 @@ static vfd_status batch_enqueue(vfd_batch *b, int n_substeps)
     for (int s = 0; s < n_substeps; ++s) {
         for (auto *w : b->worlds)
             VFD_BCUDA(b, cudaMemsetAsync(w->d_mass, 0, sizeof(double) * MS_COUNT * w->nf, b->st));
-        for (int a = 0; a < 3; ++a)
-            VFD_BCUDA(b, launch_axis(b->variant[a], b->d_jobs + a * b->njobs, b->njobs, b->tiles[a],
-                                     b->Fmax[a], b->st));
+        for (int a = 0; a < 3; ++a) {
+            if (b->use_os[a])
+                VFD_BCUDA(b, launch_os(b->d_osjobs + a * b->njobs, b->njobs, b->os_tiles[a], b->rmin[a], b->st));
+            else
+                VFD_BCUDA(b, launch_axis(b->variant[a], b->d_jobs + a * b->njobs, b->njobs, b->tiles[a],
+                                         b->Fmax[a], b->st));
+        }
     }
     for (auto *w : b->worlds)
         if (w->dep_njobs > 0)
