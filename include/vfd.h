@@ -151,6 +151,15 @@ vfd_status vfd_set_sources(vfd_world *w, int field, const int32_t *idx,
 vfd_status vfd_set_window(vfd_world *w, int field, const float *window, int kw, int kh, int kd,
                           int cx, int cy, int cz);
 
+/* Reference-mode window itself (computeKernel3D, Diffusion.cu:1078-1531):
+ * the 7-point stencil (centre 1 - 6 lambda - gamma_dt, six arms lambda)
+ * applied n_steps times to a unit impulse; out receives the centred window
+ * of half-width R ((2R+1)^3 floats, x fastest, centre at (R, R, R)).
+ * Computed on `device` as the inverse 3D FFT of the stencil spectrum to the
+ * power n_steps.  The reference's human-VF setting is lambda = 2*15/15^2,
+ * n_steps = 894, R = 73 (DiffusionHelper.cpp:48-100). */
+vfd_status vfd_stencil_window(double lambda, double gamma_dt, int n_steps, int R, float *out, int device);
+
 /* ---- one tick: n_substeps diffusion substeps of every field, then the
  * registered sources are deposited and the FP64 totals are formed.
  * Replaces fftDiffuse3D (Diffusion.cu:1622-1934) for every chemical plus
@@ -184,6 +193,62 @@ vfd_status vfd_batch_tick(vfd_batch *b, int n_substeps, void *stream);
 vfd_status vfd_batch_destroy(vfd_batch *b);
 const char *vfd_batch_last_error(const vfd_batch *b);
 
+/* ---- serving: a request loop with continuous batching --------------------
+ * Requests are queued from any thread.  One scheduler thread per server
+ * admits them in FIFO order while a slot (max_active) is free and the
+ * request's device bytes fit hbm_budget_bytes; admitted fields stay resident
+ * on the device for all the request's ticks.  Each round advances every
+ * active request by one tick (substeps_per_tick substeps) with all their
+ * fields in one launch per axis pass; finished requests are retired (totals,
+ * optional download) and free their slot and memory for the next admission.
+ * A request's results do not depend on which other requests share its
+ * rounds (each field's lines stay in their own tiles).
+ * Host buffers named by a request (init, result, mass) must stay valid until
+ * the request completes; source arrays are copied at submit. */
+typedef struct vfd_server vfd_server;
+
+typedef struct vfd_request_desc {
+    int nx, ny, nz, n_fields;
+    const vfd_field_params *fields;    /* n_fields                          */
+    int pad_mode, epi_boundary;
+    int ticks;                          /* ticks while resident               */
+    const float *const *init;           /* n_fields host fields, or NULL      */
+    uint64_t synth_seed;                /* init == NULL: vfd_synth_field_device */
+    int synth_world;                    /*   with (seed, world, field)         */
+    float synth_lo, synth_hi;
+    const int32_t *const *src_idx;      /* per field, or NULL (no sources)    */
+    const float *const *src_amt;
+    const int64_t *n_src;
+    float *const *result;               /* n_fields host buffers, or NULL     */
+    vfd_mass *mass;                     /* n_fields, or NULL                  */
+} vfd_request_desc;
+
+typedef struct vfd_request_info {
+    uint64_t id;
+    int status;                         /* vfd_status; -1 while pending       */
+    double t_submit, t_admit, t_done;   /* seconds on the server clock        */
+    double voxel_steps;
+} vfd_request_info;
+
+typedef struct vfd_server_stats {
+    int64_t submitted, admitted, completed, rejected, active, queued, rounds;
+    double busy_s;                      /* time with at least one active request */
+    double voxel_steps_done;
+    double p50_latency_s, p99_latency_s, mean_latency_s;  /* submit -> done   */
+    size_t hbm_in_use, hbm_peak;
+} vfd_server_stats;
+
+vfd_status vfd_server_create(int device, size_t hbm_budget_bytes, int max_active, int substeps_per_tick,
+                             vfd_server **out);
+vfd_status vfd_server_submit(vfd_server *s, const vfd_request_desc *req, uint64_t *id);
+/* Waits for request id; returns its status (VFD_ERR_TIMEOUT if not done). */
+vfd_status vfd_server_wait(vfd_server *s, uint64_t id, double timeout_s, vfd_request_info *info);
+vfd_status vfd_server_drain(vfd_server *s, double timeout_s);
+vfd_status vfd_server_get_stats(vfd_server *s, vfd_server_stats *out);
+double vfd_server_clock(const vfd_server *s);
+/* Stops the scheduler; requests still queued or resident are dropped. */
+vfd_status vfd_server_destroy(vfd_server *s);
+
 /* ---- per-kernel timing (the reference's PROFILE_GPU stage timers,
  * Diffusion.cu:1908-1912, as CUDA events) ---------------------------------
  * When enabled, every launch of this world is bracketed by CUDA events on
@@ -207,6 +272,9 @@ uint64_t vfd_kernel_launch_count(void);
  * replacement, strengths lognormal(mu, sigma) through FP64 Box-Muller. */
 vfd_status vfd_synth_field(uint64_t seed, int world, int field, float lo, float hi,
                            float *out, size_t n);
+/* Same values as vfd_synth_field, generated on the device into dptr. */
+vfd_status vfd_synth_field_device(uint64_t seed, int world, int field, float lo, float hi,
+                                  float *dptr, size_t n, void *stream);
 vfd_status vfd_synth_sources(uint64_t seed, int world, int field, int64_t n,
                              int64_t n_voxels, double mu, double sigma,
                              int32_t *idx, float *amt);

@@ -45,14 +45,16 @@ def test_batch_matches_single_worlds_and_oracle(gpu):
     for s in singles:
         s.tick(3)
         s.tick(3)
+    errs = []
     for i, (g, sig) in enumerate(specs):
         for f in range(3):
             got = worlds[i].download(f)
             ref_single = singles[i].download(f)
-            assert rel_l2(got, ref_single) <= 1e-6, (i, f)
             u, idx, amt = inputs[i][f]
             ref = oracle.tick(oracle.tick(u, sig[f], dec[f], 3, idx, amt), sig[f], dec[f], 3, idx, amt)
-            assert rel_l2(got, ref) <= 1e-5, (i, f)
+            errs.append((i, f, rel_l2(got, ref_single), rel_l2(got, ref), rel_l2(ref_single, ref)))
+    for e in errs:
+        assert e[2] <= 1e-6 and e[3] <= 1e-5 and e[4] <= 1e-5, errs
         m = worlds[i].mass()
         for f in range(3):
             s_ = worlds[i].download(f).astype(np.float64).sum()
@@ -77,3 +79,18 @@ def test_batch_recaptures_when_sources_change(gpu):
     del before
     w1.close()
     w2.close()
+
+
+@pytest.mark.parametrize("grid,sig", [((128, 96, 96), (0.9, 1.3, 2.4)), ((96, 64, 64), (1.0, 2.1, 0.6)),
+                                      ((512, 64, 40), (1.8, 1.8, 1.8))])
+def test_single_world_is_deterministic(gpu, grid, sig):
+    """No sources (atomics aside, every output is computed by one thread):
+    two runs on identical inputs are bitwise equal."""
+    outs = []
+    for _ in range(2):
+        w, _ = make_world(grid, sig, [0.05, 0.01, 0.03], 4, 0, n_src=0)
+        w.tick(3)
+        outs.append([w.download(f) for f in range(3)])
+        w.close()
+    for f in range(3):
+        np.testing.assert_array_equal(outs[0][f], outs[1][f])

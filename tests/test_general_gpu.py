@@ -149,3 +149,13 @@ def test_against_reference_kernels_and_cufft(gpu, kind):
     if kind == "gaussian":
         sep, _, _ = run(vfd.METHOD_SEPARABLE, grid, [sig], [0.0], ins, pad_mode=1, epi=epi, base=[base])
         assert rel_l2(sep[0], ref) <= REL_L2
+
+
+@pytest.mark.parametrize("lam,n,R", [(0.1333, 30, 12), (0.0667, 60, 14), (0.1, 7, 9)])
+def test_stencil_window_on_device(gpu, lam, n, R):
+    """vfd_stencil_window (spectrum power + inverse FFT on the device) equals
+    the explicit stencil iteration of the oracle."""
+    got = vfd.stencil_window(lam, 0.0, n, R)
+    ref = oracle.stencil_power(lam, 0.0, n, R)
+    assert float(np.abs(got - ref).max()) <= 1e-6 * float(ref.max())
+    assert abs(float(got.astype(np.float64).sum()) - float(ref.sum())) <= 1e-5

@@ -316,6 +316,37 @@ __global__ void outer_spectrum_kernel(float2 *K, const float *sx, const float *s
     }
 }
 
+// Half spectrum of the 7-point stencil to the power n on a periodic G^3 grid:
+// S(k) = c + 2 lambda (cos kx + cos ky + cos kz), c = 1 - 6 lambda - gamma dt
+// (the stencil of Diffusion.cu:1182-1195), FP64, stored FP32.
+__global__ void stencil_spectrum_kernel(float2 *K, int G, double lambda, double centre, int n)
+{
+    const int Gh = G / 2 + 1;
+    const int64_t total = (int64_t)Gh * G * G;
+    const double w = 2.0 / (double)G;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int kx = (int)(i % Gh);
+        const int64_t r = i / Gh;
+        const int ky = (int)(r % G), kz = (int)(r / G);
+        const double s = centre + 2.0 * lambda * (cospi(w * kx) + cospi(w * ky) + cospi(w * kz));
+        K[i] = make_float2((float)pow(s, (double)n), 0.0f);
+    }
+}
+
+// Centred (2R+1)^3 window of the periodic grid P (index 0 = the impulse).
+__global__ void crop_window_kernel(float *w, const float *P, int G, int R, float scale)
+{
+    const int k = 2 * R + 1;
+    const int64_t total = (int64_t)k * k * k;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % k);
+        const int64_t r = i / k;
+        const int y = (int)(r % k), z = (int)(r / k);
+        const int px = (x - R + G) % G, py = (y - R + G) % G, pz = (z - R + G) % G;
+        w[i] = scale * P[(int64_t)px + (int64_t)G * (py + (int64_t)G * pz)];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Launchers (variant = index into VFD_AXIS_VARIANTS, NL must be 16 for c2c
 // coalescing; any variant works for the row passes).
@@ -432,6 +463,21 @@ cudaError_t launch_outer_spectrum(float2 *K, const float *sx, const float *sy, c
 {
     const int Fxh = Fx / 2 + 1;
     outer_spectrum_kernel<<<grid_for((int64_t)Fxh * Fy * Fz), 256, 0, st>>>(K, sx, sy, sz, Fx, Fy, Fz, Fxh);
+    note_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stencil_spectrum(float2 *K, int G, double lambda, double centre, int n, cudaStream_t st)
+{
+    stencil_spectrum_kernel<<<grid_for((int64_t)(G / 2 + 1) * G * G), 256, 0, st>>>(K, G, lambda, centre, n);
+    note_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crop_window(float *w, const float *P, int G, int R, float scale, cudaStream_t st)
+{
+    const int64_t k = 2 * R + 1;
+    crop_window_kernel<<<grid_for(k * k * k), 256, 0, st>>>(w, P, G, R, scale);
     note_launch();
     return cudaGetLastError();
 }

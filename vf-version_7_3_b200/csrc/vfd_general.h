@@ -58,6 +58,8 @@ cudaError_t launch_crop(float *u, const float *P, int nx, int ny, int nz, int Fx
 cudaError_t launch_sum(const float *P, int64_t n, double *out, cudaStream_t st);
 cudaError_t launch_outer_spectrum(float2 *K, const float *sx, const float *sy, const float *sz, int Fx, int Fy,
                                   int Fz, cudaStream_t st);
+cudaError_t launch_stencil_spectrum(float2 *K, int G, double lambda, double centre, int n, cudaStream_t st);
+cudaError_t launch_crop_window(float *w, const float *P, int G, int R, float scale, cudaStream_t st);
 cudaError_t launch_wrap_window(float *P, const float *w, int kw, int kh, int kd, int cx, int cy, int cz, int Fx,
                                int Fy, int Fz, cudaStream_t st);
 

@@ -48,6 +48,8 @@ cudaError_t launch_axis(int variant, const AxisJob *jobs, int njobs, int tiles, 
 cudaError_t launch_deposit(const DepositJob *jobs, int njobs, const int32_t *idx, const float *amt,
                            int64_t total, int *err, cudaStream_t st);
 
+cudaError_t launch_synth_field(uint64_t key, double lo, double span, float *out, int64_t n, cudaStream_t st);
+
 void note_launch();
 
 }  // namespace vfd

@@ -307,6 +307,37 @@ __global__ void __launch_bounds__(256) deposit_kernel(const DepositJob *__restri
 }
 
 // ---------------------------------------------------------------------------
+// Device copy of the synthetic field generator (vfd_synth_field): the same
+// splitmix64 stream and the same IEEE double operations (no contraction), so
+// host and device produce identical fields.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t d_mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+__global__ void synth_field_kernel(uint64_t key, double lo, double span, float *out, int64_t n)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t z = d_mix64(key + ((uint64_t)i + 1) * 0x9e3779b97f4a7c15ULL);
+        const double u = __dmul_rn((double)(z >> 11), 1.0 / 9007199254740992.0);
+        out[i] = (float)__dadd_rn(lo, __dmul_rn(span, u));
+    }
+}
+
+cudaError_t launch_synth_field(uint64_t key, double lo, double span, float *out, int64_t n, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    int64_t blocks = (n + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    synth_field_kernel<<<(unsigned)blocks, 256, 0, st>>>(key, lo, span, out, n);
+    note_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Launch wrappers
 // ---------------------------------------------------------------------------
 template <int NL, int TL, int MAXP, int MINB>

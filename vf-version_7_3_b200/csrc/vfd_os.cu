@@ -15,7 +15,11 @@
 // Work split: a CTA owns 32 real lines (16 complex pairs: line q is the real
 // part of pair q % 16 for q < 16, the imaginary part otherwise -- the kernel
 // spectrum is real and even, so the pair's parts are convolved independently)
-// and a chunk of OS_M consecutive blocks of those lines.  A group of 8 lanes
+// over their whole length, processed in chunks of M consecutive blocks.  The
+// field is updated in place: a chunk's 2r-sample input halo that overlaps
+// the previous chunk's outputs is carried forward in shared memory before
+// those outputs are stored, so no CTA ever reads a sample another chunk has
+// already overwritten (and no two CTAs share a line).  A group of 8 lanes
 // computes one (pair, block) FFT: lane t holds samples t + 8q (q = 0..7);
 //   forward : DFT-8 over q in registers, twiddle w64^(t k1), transpose
 //             through a swizzled per-group scratch (__syncwarp only), DFT-8
@@ -26,6 +30,7 @@
 // staging as the full-line kernel (conflict-free for the group pattern used).
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include "vfd_internal.h"
 #include "vfd_os.h"
@@ -90,7 +95,8 @@ __device__ __forceinline__ void fft64_inv(float2 (&x)[8], int t, float2 *scr, co
     Dft<8, true>::run(x);
 }
 
-__global__ void __launch_bounds__(OS_NT, 2) os_pass_kernel(const OsJob *__restrict__ jobs, int njobs)
+template <int M, int MINB>
+__global__ void __launch_bounds__(OS_NT, MINB) os_pass_kernel(const OsJob *__restrict__ jobs, int njobs)
 {
     extern __shared__ __align__(16) float2 osm[];
     __shared__ double red[OS_NT / 32];
@@ -108,149 +114,209 @@ __global__ void __launch_bounds__(OS_NT, 2) os_pass_kernel(const OsJob *__restri
         sj = jobs[lo];
     }
     if (threadIdx.x < 64) {
-        double s, c;
-        sincospi((double)threadIdx.x / 32.0, &s, &c);
-        tw64[threadIdx.x] = make_float2((float)c, (float)-s);
+        double sn, cs;
+        sincospi((double)threadIdx.x / 32.0, &sn, &cs);
+        tw64[threadIdx.x] = make_float2((float)cs, (float)-sn);
     }
     __syncthreads();
 
     const int n = sj.n, r = sj.r, L = sj.L, C = sj.C;
-    const int NP = C + 2 * r;                 // staged input positions
+    const int NP = C + 2 * r;                 // staged input positions per chunk
     float2 *in = osm;                         // [NP][OS_LS]
     float2 *out = in + NP * OS_LS;            // [C][OS_LS]
     float2 *scr = out + C * OS_LS;            // [32 groups][OS_SCR]
     float *inf = reinterpret_cast<float *>(in);
     float *outf = reinterpret_cast<float *>(out);
 
+    // this CTA owns 32 lines of one outer index, whole length, all chunks
     const int local = tile - sj.tile_begin;
     const int outer = local / sj.tiles_per_outer;
-    const int q0 = local - outer * sj.tiles_per_outer;
-    const int lt = q0 / sj.nchunks, ch = q0 - lt * sj.nchunks;
+    const int lt = local - outer * sj.tiles_per_outer;
     const int l0 = lt * 32;
     const int nreal = min(32, sj.nlines - l0);
-    const int c0 = -r + ch * C;               // first output position of the chunk
-    const int p0 = c0 - r;                    // first staged input position
     float *base = sj.data + outer * sj.outer_stride + (int64_t)l0 * sj.line_stride;
     const int kind = sj.kind;
     const float b = sj.b;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int NW = OS_NT / 32;
 
-    // ---- stage the input chunk (padding rule fused into the x pass) -----
-    double acc_in = 0.0;
-    if (kind == PASS_X) {
-        // lane = position along the row: 128-byte coalesced reads
-        const int xlo = sj.box_lo[0], xhi = sj.box_hi[0];
-        for (int row = warp; row < 32; row += OS_NT / 32) {
-            bool rowin = false;
-            if (row < nreal) {
-                const int rr = l0 + row;
-                const int y = rr % sj.ny, z = rr / sj.ny;
-                rowin = y >= sj.box_lo[1] && y < sj.box_hi[1] && z >= sj.box_lo[2] && z < sj.box_hi[2];
-            }
-            const float *src = base + (int64_t)row * sj.line_stride;
-            const int sidx = 2 * (row & 15) + (row >> 4);
-            constexpr int U = 4;
-            for (int i0 = lane; i0 < NP; i0 += 32 * U) {
-                float v[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int i = i0 + 32 * u, p = p0 + i;
-                    v[u] = (rowin && i < NP && p >= 0 && p < n) ? __ldg(src + p) : 0.0f;
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int i = i0 + 32 * u, p = p0 + i;
-                    if (i < NP) {
-                        const float x = (rowin && p >= xlo && p < xhi) ? v[u] - b : 0.0f;
-                        inf[i * 2 * OS_LS + sidx] = x;
-                        if (p >= c0 && p < c0 + C) acc_in += (double)x;
-                    }
-                }
-            }
-        }
-    } else {
-        // lane = column: 128-byte coalesced reads of one position
-        const int64_t ps = sj.pos_stride;
-        const int sidx = 2 * (lane & 15) + (lane >> 4);
-        const bool ok = lane < nreal;
-        const float *src = base + (int64_t)lane * sj.line_stride;
-        constexpr int U = 8;
-        for (int i0 = warp; i0 < NP; i0 += (OS_NT / 32) * U) {
-            float v[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int i = i0 + (OS_NT / 32) * u, p = p0 + i;
-                v[u] = (ok && i < NP && p >= 0 && p < n) ? __ldg(src + p * ps) : 0.0f;
-            }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int i = i0 + (OS_NT / 32) * u;
-                if (i < NP) inf[i * 2 * OS_LS + sidx] = v[u];
-            }
-        }
-    }
-    __syncthreads();
-
-    // ---- blocks: FFT-64, multiply, inverse, keep L samples ----------------
+    // per-lane constants of the FFT phase
     const int g = threadIdx.x >> 3, t = threadIdx.x & 7;
     float2 *gs = scr + g * OS_SCR;
     float2 w[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) w[k] = tw64[(t * k) & 63];
-    float H[8];
+    unsigned qmask = 0;  // samples t + 8q that are outputs of a block
 #pragma unroll
-    for (int k = 0; k < 8; ++k) H[k] = sj.H[t + 8 * k];
-    double acc_leak = 0.0;
-    const int nitems = OS_PAIRS * OS_M;
-    for (int u = g; u < nitems; u += OS_NT / 8) {
-        // groups 2j, 2j+1 of a warp take pairs p, p + 8 (conflict-free staging reads)
-        const int pair = ((u & 1) << 3) | ((u >> 1) & 7);
-        const int blk = u >> 4;
-        const int seg0 = blk * L;
-        float2 x[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) x[q] = in[(seg0 + t + 8 * q) * OS_LS + pair];
-        fft64_fwd(x, t, gs, w);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) x[k] = make_float2(x[k].x * H[k], x[k].y * H[k]);
-        fft64_inv(x, t, gs, w);
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int i = t + 8 * q;
-            if (i >= r && i < r + L) {
-                const int j = seg0 + i - r;   // chunk output index
-                const int o = c0 + j;
-                if (o >= 0 && o < n) out[j * OS_LS + pair] = x[q];
-                else acc_leak += (double)x[q].x + (double)x[q].y;
-            }
+    for (int q = 0; q < 8; ++q) {
+        const int i = t + 8 * q;
+        if (i >= r && i < r + L) qmask |= 1u << q;
+    }
+
+    // x-pass row state (lane = position; rows = lines of the tile)
+    int xlo = 0, xhi = 0;
+    unsigned rowin_mask = 0;  // bit row: row inside the padding rule's y/z range
+    if (kind == PASS_X) {
+        xlo = sj.box_lo[0];
+        xhi = sj.box_hi[0];
+        for (int row = 0; row < nreal; ++row) {
+            const int rr = l0 + row;
+            const int y = rr % sj.ny, z = rr / sj.ny;
+            if (y >= sj.box_lo[1] && y < sj.box_hi[1] && z >= sj.box_lo[2] && z < sj.box_hi[2])
+                rowin_mask |= 1u << row;
         }
     }
-    __syncthreads();
+    const int64_t ps = sj.pos_stride;
 
-    // ---- store the chunk's outputs (baseline + decay + mass in the z pass) -
-    double acc_conv = 0.0, acc_out = 0.0;
-    const int jlo = max(0, -c0), jhi = min(C, n - c0);
-    if (kind == PASS_X) {
-        for (int row = warp; row < nreal; row += OS_NT / 32) {
-            float *dst = base + (int64_t)row * sj.line_stride + c0;
-            const int sidx = 2 * (row & 15) + (row >> 4);
-            for (int j = jlo + lane; j < jhi; j += 32) dst[j] = outf[j * 2 * OS_LS + sidx];
+    double acc_in = 0.0, acc_leak = 0.0, acc_conv = 0.0, acc_out = 0.0;
+    for (int ch = 0; ch < sj.nchunks; ++ch) {
+        const int c0 = -r + ch * C;           // first output position of the chunk
+        const int p0 = c0 - r;                // first staged input position
+        // positions [p0, p0 + 2r) were staged by the previous chunk (its last
+        // 2r slots) before it overwrote anything; bring them forward and load
+        // only the rest from global memory
+        int ifirst = 0;
+        if (ch > 0) {
+            for (int i = threadIdx.x; i < 2 * r * OS_LS; i += OS_NT) in[i] = in[C * OS_LS + i];
+            ifirst = 2 * r;
+            __syncthreads();
         }
-    } else if (lane < nreal) {
-        const int64_t ps = sj.pos_stride;
-        const int sidx = 2 * (lane & 15) + (lane >> 4);
-        float *dst = base + (int64_t)lane * sj.line_stride;
-        const bool last = kind == PASS_Z;
-        const float keep = sj.keep;
-        for (int j = jlo + warp; j < jhi; j += OS_NT / 32) {
-            float v = outf[j * 2 * OS_LS + sidx];
-            if (last) {
-                acc_conv += (double)v;
-                v = keep * (v + b);
-                acc_out += (double)v;
+        const bool in_inside = p0 + ifirst >= 0 && p0 + NP <= n;
+        // ---- stage the chunk's new input positions -------------------------
+        if (kind == PASS_X) {
+            // lane = position along the row: 128-byte coalesced reads
+            for (int row = warp; row < 32; row += NW) {
+                const bool rowin = (rowin_mask >> row) & 1u;
+                const int sidx = 2 * (row & 15) + (row >> 4);
+                const float *src = base + (int64_t)row * sj.line_stride + p0;
+                float *dst = inf + sidx;
+                const bool fast = rowin && p0 + ifirst >= xlo && p0 + NP <= xhi;
+                constexpr int U = 4;
+                for (int i0 = ifirst + lane; i0 < NP; i0 += 32 * U) {
+                    float v[U];
+                    if (fast) {
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            const int i = i0 + 32 * u;
+                            v[u] = i < NP ? __ldg(src + i) - b : 0.0f;
+                        }
+                    } else {
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            const int i = i0 + 32 * u, p = p0 + i;
+                            v[u] = (rowin && i < NP && p >= xlo && p < xhi) ? __ldg(src + i) - b : 0.0f;
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int i = i0 + 32 * u;
+                        if (i < NP) {
+                            dst[i * 2 * OS_LS] = v[u];
+                            acc_in += (double)v[u];  // every position is staged once
+                        }
+                    }
+                }
             }
-            dst[(int64_t)(c0 + j) * ps] = v;
+        } else {
+            // lane = column: 128-byte coalesced reads of one position
+            const int sidx = 2 * (lane & 15) + (lane >> 4);
+            const bool ok = lane < nreal;
+            const float *src = base + (int64_t)lane * sj.line_stride + (int64_t)(p0 + ifirst + warp) * ps;
+            const int64_t step = (int64_t)NW * ps;
+            float *dst = inf + (ifirst + warp) * 2 * OS_LS + sidx;
+            constexpr int DST = NW * 2 * OS_LS;
+            constexpr int U = 8;
+            for (int i0 = ifirst + warp; i0 < NP; i0 += NW * U) {
+                float v[U];
+                if (in_inside) {
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+                        v[u] = (ok && i0 + NW * u < NP) ? __ldg(src + u * step) : 0.0f;
+                } else {
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int p = p0 + i0 + NW * u;
+                        v[u] = (ok && i0 + NW * u < NP && p >= 0 && p < n) ? __ldg(src + u * step) : 0.0f;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (i0 + NW * u < NP) dst[u * DST] = v[u];
+                src += U * step;
+                dst += U * DST;
+            }
         }
+        __syncthreads();
+
+        // ---- blocks: FFT-64, multiply, inverse, keep L samples -------------
+        const bool out_inside = c0 >= 0 && c0 + C <= n;
+        for (int u = g; u < OS_PAIRS * M; u += OS_NT / 8) {
+            // groups 2j, 2j+1 of a warp take pairs p, p + 8 (conflict-free staging reads)
+            const int pair = ((u & 1) << 3) | ((u >> 1) & 7);
+            const int seg0 = (u >> 4) * L;
+            const float2 *sp = in + (seg0 + t) * OS_LS + pair;
+            float2 x[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) x[q] = sp[q * 8 * OS_LS];
+            fft64_fwd(x, t, gs, w);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const float h = sj.H[t + 8 * k];
+                x[k] = make_float2(x[k].x * h, x[k].y * h);
+            }
+            fft64_inv(x, t, gs, w);
+            float2 *op = out + (seg0 + t - r) * OS_LS + pair;  // sample t + 8q -> out row seg0 + t + 8q - r
+            if (out_inside) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if ((qmask >> q) & 1u) op[q * 8 * OS_LS] = x[q];
+            } else {
+                const int o0 = c0 + seg0 + t - r;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    if ((qmask >> q) & 1u) {
+                        const int o = o0 + 8 * q;
+                        if (o >= 0 && o < n) op[q * 8 * OS_LS] = x[q];
+                        else acc_leak += (double)x[q].x + (double)x[q].y;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- store the chunk's outputs (baseline + decay + mass in the z pass)
+        const int jlo = max(0, -c0), jhi = min(C, n - c0);
+        if (kind == PASS_X) {
+            for (int row = warp; row < nreal; row += NW) {
+                float *dst = base + (int64_t)row * sj.line_stride + c0;
+                const float *sv = outf + 2 * (row & 15) + (row >> 4);
+                for (int j = jlo + lane; j < jhi; j += 32) dst[j] = sv[j * 2 * OS_LS];
+            }
+        } else if (lane < nreal) {
+            const float *sv = outf + (jlo + warp) * 2 * OS_LS + 2 * (lane & 15) + (lane >> 4);
+            float *dst = base + (int64_t)lane * sj.line_stride + (int64_t)(c0 + jlo + warp) * ps;
+            const int64_t step = (int64_t)NW * ps;
+            if (kind == PASS_Z) {
+                const float keep = sj.keep;
+                for (int j = jlo + warp; j < jhi; j += NW) {
+                    float v = *sv;
+                    acc_conv += (double)v;
+                    v = keep * (v + b);
+                    acc_out += (double)v;
+                    *dst = v;
+                    sv += NW * 2 * OS_LS;
+                    dst += step;
+                }
+            } else {
+                for (int j = jlo + warp; j < jhi; j += NW) {
+                    *dst = *sv;
+                    sv += NW * 2 * OS_LS;
+                    dst += step;
+                }
+            }
+        }
+        // the next chunk's halo copy reads `in` (no longer read by the FFT
+        // phase) and its FFT phase writes `out` only after the next barrier
     }
 
     double *mass = sj.mass;
@@ -266,27 +332,44 @@ __global__ void __launch_bounds__(OS_NT, 2) os_pass_kernel(const OsJob *__restri
     }
 }
 
-size_t os_smem_bytes(int rmin)
+int os_blocks_per_chunk()
 {
-    const int L = OS_N - 2 * rmin, C = OS_M * L;
+    static int m = -1;
+    if (m < 0) {
+        const char *e = getenv("VFD_OS_M");
+        m = (e && e[0] == '4') ? 4 : 2;
+    }
+    return m;
+}
+
+size_t os_smem_bytes(int rmin, int M)
+{
+    const int L = OS_N - 2 * rmin, C = M * L;
     return ((size_t)(C + 2 * rmin) * OS_LS + (size_t)C * OS_LS + (size_t)(OS_NT / 8) * OS_SCR) * sizeof(float2);
+}
+
+template <int M, int MINB>
+static cudaError_t launch_os_t(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st)
+{
+    static thread_local int configured_dev = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured_dev != dev) {
+        cudaError_t e = cudaFuncSetAttribute(os_pass_kernel<M, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)axis_smem_limit());
+        if (e != cudaSuccess) return e;
+        configured_dev = dev;
+    }
+    os_pass_kernel<M, MINB><<<tiles, OS_NT, os_smem_bytes(rmin, M), st>>>(jobs, njobs);
+    note_launch();
+    return cudaGetLastError();
 }
 
 cudaError_t launch_os(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st)
 {
     if (tiles <= 0) return cudaSuccess;
-    static thread_local int configured_dev = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_dev != dev) {
-        cudaError_t e = cudaFuncSetAttribute(os_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)axis_smem_limit());
-        if (e != cudaSuccess) return e;
-        configured_dev = dev;
-    }
-    os_pass_kernel<<<tiles, OS_NT, os_smem_bytes(rmin), st>>>(jobs, njobs);
-    note_launch();
-    return cudaGetLastError();
+    if (os_blocks_per_chunk() == 4) return launch_os_t<4, 2>(jobs, njobs, tiles, rmin, st);
+    return launch_os_t<2, 3>(jobs, njobs, tiles, rmin, st);
 }
 
 }  // namespace vfd

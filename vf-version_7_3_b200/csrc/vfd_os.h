@@ -8,11 +8,10 @@
 namespace vfd {
 
 constexpr int OS_N = 64;      // FFT length of one overlap-save block
-constexpr int OS_M = 4;       // blocks per CTA chunk
 constexpr int OS_RMAX = 16;   // largest kernel radius (L = 64 - 2r >= 32)
 
 // One (field, axis) pass; line addressing as in AxisJob.  A tile is 32 real
-// lines x one chunk of OS_M blocks; tiles are ordered (outer, line tile, chunk).
+// lines of one outer index over their whole length (all chunks, in order).
 struct OsJob {
     float *data;
     double *mass;
@@ -20,7 +19,7 @@ struct OsJob {
     int n, nlines, nouter;
     int r, L, C;           // kernel radius, outputs per block (64 - 2r), outputs per chunk
     int nchunks;           // ceil((n + 2r) / C): chunks cover outputs [-r, n + r)
-    int tiles_per_outer;   // ceil(nlines / 32) * nchunks
+    int tiles_per_outer;   // ceil(nlines / 32)
     int tile_begin;
     int kind;              // PassKind
     float b, keep;
@@ -29,7 +28,10 @@ struct OsJob {
     float H[OS_N];         // G64(k) / 64, FP64-generated
 };
 
-size_t os_smem_bytes(int rmin);
+// Blocks per CTA chunk (2 by default, 4 with VFD_OS_M=4); jobs must be built
+// with the same value.
+int os_blocks_per_chunk();
+size_t os_smem_bytes(int rmin, int M);
 cudaError_t launch_os(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st);
 
 }  // namespace vfd

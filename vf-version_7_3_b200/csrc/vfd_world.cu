@@ -371,9 +371,9 @@ static OsJob make_os_job(const vfd_world *w, int f, int a, int tile_begin)
     j.nouter = aj.nouter;
     j.r = w->params[f].radius[a];
     j.L = OS_N - 2 * j.r;
-    j.C = OS_M * j.L;
+    j.C = os_blocks_per_chunk() * j.L;
     j.nchunks = (j.n + 2 * j.r + j.C - 1) / j.C;
-    j.tiles_per_outer = ((j.nlines + 31) / 32) * j.nchunks;
+    j.tiles_per_outer = (j.nlines + 31) / 32;
     j.tile_begin = tile_begin;
     j.kind = a;
     j.b = aj.b;
@@ -1390,6 +1390,101 @@ vfd_status vfd_batch_tick(vfd_batch *b, int n_substeps, void *stream)
 const char *vfd_batch_last_error(const vfd_batch *b) { return b ? b->err.c_str() : g_thread_error.c_str(); }
 
 // ---------------------------------------------------------------------------
+// Reference-mode kernel construction (computeKernel3D, Diffusion.cu:1078-1531).
+// The reference raises the 7-point stencil to the power n by repeated FFT
+// convolution (niter rounds of complexPower on a 616^3 grid with a 299^3
+// crop between rounds) and keeps the centred window.  Here the power is
+// taken once in the frequency domain on a periodic G^3 grid, G >= 2R + 1 +
+// 16 sigma (sigma^2 = 2 lambda n per axis), so the wrapped tails that reach
+// the window are below FP32 resolution, then one inverse 3D FFT and the crop.
+// (The reference's complexPower uses atanf(b/a), which drops the sign of
+// bins with a negative real part; those bins have |S|^n < 1e-30 at the
+// reference's lambda, so the two agree to FP32 resolution.)
+// ---------------------------------------------------------------------------
+vfd_status vfd_stencil_window(double lambda, double gamma_dt, int n_steps, int R, float *out, int device)
+{
+    if (!out || R < 0 || n_steps < 0 || !(lambda >= 0.0) || lambda > 1.0 / 6.0)
+        return fail(nullptr, VFD_ERR_INVALID_ARG, "bad stencil parameters (0 <= lambda <= 1/6, R >= 0)");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(nullptr, VFD_ERR_NO_DEVICE, "no device");
+    const double sigma = std::sqrt(2.0 * lambda * (double)n_steps);
+    int G = -1;
+    for (int g = 2 * R + 2 + 2 * (int)std::ceil(8.0 * sigma); g < 4096; ++g) {
+        if (g & 1) continue;
+        FftPlan p;
+        if (make_plan(g, &p) && any_variant_fits(p) && pick_variant(std::vector<FftPlan>{p}, 16) >= 0) {
+            G = g;
+            break;
+        }
+    }
+    if (G < 0) return fail(nullptr, VFD_ERR_NOT_SUPPORTED, "stencil window too wide for the device FFT");
+    DeviceGuard dg(device);
+    FftPlan plan;
+    make_plan(G, &plan);
+    const int vrow = pick_variant(std::vector<FftPlan>{plan});
+    const int vcol = pick_variant(std::vector<FftPlan>{plan}, 16);
+    const int Gh = G / 2 + 1;
+    const int64_t nk = (int64_t)Gh * G * G, np = (int64_t)G * G * G, nw = (int64_t)(2 * R + 1) * (2 * R + 1) * (2 * R + 1);
+    float2 *K = nullptr, *tw = nullptr;
+    float *P = nullptr, *W = nullptr;
+    std::vector<float2> htw;
+    twiddles(G, htw);
+    cudaError_t e = cudaSuccess;
+    auto run = [&]() -> cudaError_t {
+        cudaError_t r;
+        if ((r = cudaMalloc(&K, sizeof(float2) * nk)) != cudaSuccess) return r;
+        if ((r = cudaMalloc(&P, sizeof(float) * np)) != cudaSuccess) return r;
+        if ((r = cudaMalloc(&W, sizeof(float) * nw)) != cudaSuccess) return r;
+        if ((r = cudaMalloc(&tw, sizeof(float2) * G)) != cudaSuccess) return r;
+        if ((r = cudaMemcpy(tw, htw.data(), sizeof(float2) * G, cudaMemcpyHostToDevice)) != cudaSuccess) return r;
+        if ((r = launch_stencil_spectrum(K, G, lambda, 1.0 - 6.0 * lambda - gamma_dt, n_steps, 0)) != cudaSuccess)
+            return r;
+        GenColPass c;
+        memset(&c, 0, sizeof(c));
+        c.plan = plan;
+        c.tw = tw;
+        c.data = K;
+        c.nlines = Gh;
+        c.scale = 1.0f;
+        c.mode = GEN_INVERSE;
+        c.nload = c.nstore = G;
+        // z lines: outer = y
+        c.nouter = G;
+        c.outer_stride = Gh;
+        c.pos_stride = (int64_t)G * Gh;
+        if ((r = launch_gen_cols(vcol, c, 0)) != cudaSuccess) return r;
+        // y lines: outer = z
+        c.outer_stride = (int64_t)G * Gh;
+        c.pos_stride = Gh;
+        if ((r = launch_gen_cols(vcol, c, 0)) != cudaSuccess) return r;
+        GenRowPass rp;
+        memset(&rp, 0, sizeof(rp));
+        rp.plan = plan;
+        rp.tw = tw;
+        rp.nrows = G * G;
+        rp.rows_per_plane = G;
+        rp.r_s1 = G;
+        rp.r_s2 = (int64_t)G * G;
+        rp.c_s1 = Gh;
+        rp.c_s2 = (int64_t)Gh * G;
+        rp.nstore = G;
+        rp.rdst = P;
+        rp.csrc = K;
+        if ((r = launch_gen_rows(vrow, rp, true, 0)) != cudaSuccess) return r;
+        if ((r = launch_crop_window(W, P, G, R, (float)(1.0 / (double)np), 0)) != cudaSuccess) return r;
+        return cudaMemcpy(out, W, sizeof(float) * nw, cudaMemcpyDeviceToHost);
+    };
+    e = run();
+    cudaFree(K);
+    cudaFree(P);
+    cudaFree(W);
+    cudaFree(tw);
+    if (e != cudaSuccess) return fail(nullptr, e == cudaErrorMemoryAllocation ? VFD_ERR_OUT_OF_MEMORY : VFD_ERR_CUDA,
+                                      std::string("stencil window: ") + cudaGetErrorString(e));
+    return VFD_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Synthetic inputs: counter-based splitmix64 (Steele, Lea, Flood 2014
 // finaliser) keyed by (seed, world, field, stream).
 // ---------------------------------------------------------------------------
@@ -1418,7 +1513,20 @@ vfd_status vfd_synth_field(uint64_t seed, int world, int field, float lo, float 
     const uint64_t key = stream_key(seed, world, field, 0);
     const double a = lo, span = (double)hi - (double)lo;
 #pragma omp parallel for schedule(static)
-    for (long long i = 0; i < (long long)n; ++i) out[i] = (float)(a + span * u01(key, (uint64_t)i));
+    for (long long i = 0; i < (long long)n; ++i) {
+        volatile double prod = span * u01(key, (uint64_t)i);  // rounded product, then the sum
+        out[i] = (float)(a + prod);
+    }
+    return VFD_OK;
+}
+
+vfd_status vfd_synth_field_device(uint64_t seed, int world, int field, float lo, float hi, float *dptr, size_t n,
+                                  void *stream)
+{
+    if (!dptr && n) return fail(nullptr, VFD_ERR_INVALID_ARG, "dptr is NULL");
+    const uint64_t key = stream_key(seed, world, field, 0);
+    cudaError_t e = launch_synth_field(key, (double)lo, (double)hi - (double)lo, dptr, (int64_t)n, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail(nullptr, VFD_ERR_CUDA, std::string("synth: ") + cudaGetErrorString(e));
     return VFD_OK;
 }
 

@@ -40,7 +40,9 @@ EXPORTED = [
     "vfd_kernel_launch_count", "vfd_synth_field", "vfd_synth_sources",
     "vfd_world_set_profiling", "vfd_read_profile",
     "vfd_batch_create", "vfd_batch_tick", "vfd_batch_destroy", "vfd_batch_last_error",
-    "vfd_set_window",
+    "vfd_set_window", "vfd_synth_field_device", "vfd_stencil_window",
+    "vfd_server_create", "vfd_server_submit", "vfd_server_wait", "vfd_server_drain",
+    "vfd_server_get_stats", "vfd_server_clock", "vfd_server_destroy",
 ]
 
 
@@ -73,6 +75,32 @@ class Mass(C.Structure):
                 "sources": self.sources}
 
 
+class RequestDesc(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("n_fields", C.c_int),
+                ("fields", C.POINTER(FieldParams)), ("pad_mode", C.c_int), ("epi_boundary", C.c_int),
+                ("ticks", C.c_int), ("init", C.POINTER(C.c_void_p)), ("synth_seed", C.c_uint64),
+                ("synth_world", C.c_int), ("synth_lo", C.c_float), ("synth_hi", C.c_float),
+                ("src_idx", C.POINTER(C.c_void_p)), ("src_amt", C.POINTER(C.c_void_p)),
+                ("n_src", C.POINTER(C.c_int64)), ("result", C.POINTER(C.c_void_p)),
+                ("mass", C.POINTER(Mass))]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("status", C.c_int), ("t_submit", C.c_double),
+                ("t_admit", C.c_double), ("t_done", C.c_double), ("voxel_steps", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64),
+                ("rejected", C.c_int64), ("active", C.c_int64), ("queued", C.c_int64),
+                ("rounds", C.c_int64), ("busy_s", C.c_double), ("voxel_steps_done", C.c_double),
+                ("p50_latency_s", C.c_double), ("p99_latency_s", C.c_double),
+                ("mean_latency_s", C.c_double), ("hbm_in_use", C.c_size_t), ("hbm_peak", C.c_size_t)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def load(path=LIB_PATH):
     if not os.path.exists(path):
         raise ImportError(f"libvfd.so not built at {path}; run `make` in "
@@ -98,6 +126,17 @@ def load(path=LIB_PATH):
     lib.vfd_batch_destroy.argtypes = [P]
     lib.vfd_batch_last_error.argtypes = [P]
     lib.vfd_batch_last_error.restype = C.c_char_p
+    lib.vfd_stencil_window.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, P, C.c_int]
+    lib.vfd_synth_field_device.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_float, C.c_float, P,
+                                           C.c_size_t, P]
+    lib.vfd_server_create.argtypes = [C.c_int, C.c_size_t, C.c_int, C.c_int, C.POINTER(P)]
+    lib.vfd_server_submit.argtypes = [P, C.POINTER(RequestDesc), C.POINTER(C.c_uint64)]
+    lib.vfd_server_wait.argtypes = [P, C.c_uint64, C.c_double, C.POINTER(RequestInfo)]
+    lib.vfd_server_drain.argtypes = [P, C.c_double]
+    lib.vfd_server_get_stats.argtypes = [P, C.POINTER(ServerStats)]
+    lib.vfd_server_clock.argtypes = [P]
+    lib.vfd_server_clock.restype = C.c_double
+    lib.vfd_server_destroy.argtypes = [P]
     lib.vfd_status_string.argtypes = [C.c_int]
     lib.vfd_status_string.restype = C.c_char_p
     lib.vfd_last_error.argtypes = [P]
@@ -109,7 +148,7 @@ def load(path=LIB_PATH):
                                       C.c_double, C.c_double, P, P]
     for name in EXPORTED:
         if name not in ("vfd_status_string", "vfd_last_error", "vfd_kernel_launch_count",
-                        "vfd_batch_last_error"):
+                        "vfd_batch_last_error", "vfd_server_clock"):
             getattr(lib, name).restype = C.c_int
     return lib
 
@@ -297,6 +336,108 @@ class Batch:
     def close(self):
         if getattr(self, "_h", None):
             lib().vfd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def stencil_window(lam, gamma_dt, n_steps, R, device=0):
+    """The reference's kernel window: 7-point stencil to the power n_steps,
+    centred (2R+1)^3 window, computed on the device."""
+    w = np.empty((2 * R + 1,) * 3, np.float32)
+    _check(lib().vfd_stencil_window(lam, gamma_dt, n_steps, R, _ptr(w), device))
+    return w
+
+
+class Server:
+    """Request loop with continuous batching (vfd_server_*)."""
+
+    def __init__(self, hbm_budget_bytes, max_active, substeps_per_tick=1, device=0):
+        h = C.c_void_p()
+        _check(lib().vfd_server_create(device, int(hbm_budget_bytes), int(max_active),
+                                       int(substeps_per_tick), C.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def submit(self, grid, params, ticks, init=None, synth=None, sources=None, result=None,
+               pad_mode=PAD_ZERO, epi_boundary=0):
+        """grid (nx, ny, nz); params: list of FieldParams; init: list of host arrays or None;
+        synth: (seed, world, lo, hi) when init is None; sources: list of (idx, amt) per field;
+        result: list of host arrays receiving the final fields.  Returns the request id."""
+        nx, ny, nz = grid
+        nf = len(params)
+        keep = []
+        d = RequestDesc()
+        d.nx, d.ny, d.nz, d.n_fields = nx, ny, nz, nf
+        fp = (FieldParams * nf)(*params)
+        keep.append(fp)
+        d.fields = C.cast(fp, C.POINTER(FieldParams))
+        d.pad_mode, d.epi_boundary, d.ticks = pad_mode, epi_boundary, int(ticks)
+        if init is not None:
+            arrs = [np.ascontiguousarray(a, np.float32) for a in init]
+            keep.append(arrs)
+            ip = (C.c_void_p * nf)(*[a.ctypes.data for a in arrs])
+            keep.append(ip)
+            d.init = C.cast(ip, C.POINTER(C.c_void_p))
+        else:
+            seed, world, lo, hi = synth
+            d.synth_seed, d.synth_world, d.synth_lo, d.synth_hi = seed, world, lo, hi
+        if sources is not None:
+            idxs = [np.ascontiguousarray(i, np.int32) for i, _ in sources]
+            amts = [np.ascontiguousarray(a, np.float32) for _, a in sources]
+            ns = (C.c_int64 * nf)(*[i.size for i in idxs])
+            pi = (C.c_void_p * nf)(*[i.ctypes.data for i in idxs])
+            pa = (C.c_void_p * nf)(*[a.ctypes.data for a in amts])
+            keep += [idxs, amts, ns, pi, pa]
+            d.src_idx = C.cast(pi, C.POINTER(C.c_void_p))
+            d.src_amt = C.cast(pa, C.POINTER(C.c_void_p))
+            d.n_src = C.cast(ns, C.POINTER(C.c_int64))
+        if result is not None:
+            rp = (C.c_void_p * nf)(*[a.ctypes.data for a in result])
+            keep += [result, rp]
+            d.result = C.cast(rp, C.POINTER(C.c_void_p))
+        m = (Mass * nf)()
+        keep.append(m)
+        d.mass = C.cast(m, C.POINTER(Mass))
+        rid = C.c_uint64()
+        _check(lib().vfd_server_submit(self._h, C.byref(d), C.byref(rid)))
+        self._keep[rid.value] = (keep, m)
+        return rid.value
+
+    def wait(self, rid, timeout_s=600.0):
+        info = RequestInfo()
+        st = lib().vfd_server_wait(self._h, rid, timeout_s, C.byref(info))
+        if st != 0:
+            raise VfdError(st, f"request {rid}")
+        keep, m = self._keep.pop(rid)
+        out = {k: getattr(info, k) for k, _ in info._fields_}
+        out["mass"] = [x.as_dict() for x in m]
+        return out
+
+    def drain(self, timeout_s=600.0):
+        _check(lib().vfd_server_drain(self._h, timeout_s))
+
+    def stats(self):
+        st = ServerStats()
+        _check(lib().vfd_server_get_stats(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def clock(self):
+        return lib().vfd_server_clock(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().vfd_server_destroy(self._h)
             self._h = None
 
     def __del__(self):
