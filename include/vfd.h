@@ -249,6 +249,30 @@ double vfd_server_clock(const vfd_server *s);
 /* Stops the scheduler; requests still queued or resident are dropped. */
 vfd_status vfd_server_destroy(vfd_server *s);
 
+/* ---- allocation-free single-field transform -------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (they manage all device memory in their own arena or pool, or must not
+ * trigger the device-wide synchronisation that cudaMalloc / cudaFree can
+ * cause inside a per-tick loop): one substep of the general 3D FFT
+ * convolution of one field, in place,
+ *     field <- keep * (baseline * kernel_sum + conv(M .* (field - baseline)))
+ * (the VFD_METHOD_FFT3D transform; M and baseline as in vfd_pad_mode), where
+ * kspec is the unscaled spectrum of the wrapped kernel window on the
+ * fx * fy * fz grid, laid out [fz][fy][fx/2 + 1] as interleaved (re, im)
+ * floats -- the layout of the reference's d_KernelSpectrum -- and
+ * kernel_sum = Re kspec[0].  field and kspec are device pointers; fx must be
+ * even and each F >= n + the window's half-width; lengths 7-smooth.
+ * Allocates nothing: its scratch (the pruned field spectrum, nz*fy*(fx/2+1)
+ * complex values, plus twiddles) lives in a fixed 32 MiB __device__ array
+ * held by every GPU that loads the library; larger problems return
+ * VFD_ERR_INVALID_ARG.  The first call on a device looks up that array's
+ * address (make it before any stream capture).  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller.
+ * Asynchronous on `stream`. */
+vfd_status vfd_fft_diffuse3d_noalloc(float *field, const float *kspec, int nx, int ny, int nz,
+                                     int fx, int fy, int fz, int pad_mode, int epi_boundary,
+                                     float baseline, float kernel_sum, float keep, void *stream);
+
 /* ---- per-kernel timing (the reference's PROFILE_GPU stage timers,
  * Diffusion.cu:1908-1912, as CUDA events) ---------------------------------
  * When enabled, every launch of this world is bracketed by CUDA events on

@@ -50,6 +50,11 @@ cudaError_t launch_deposit(const DepositJob *jobs, int njobs, const int32_t *idx
 
 cudaError_t launch_synth_field(uint64_t key, double lo, double span, float *out, int64_t n, cudaStream_t st);
 
+// FFT plan of length F (radices 8,7,5,4,3,2) that some kernel variant can run,
+// and the preferred variant for it (need_nl = 0: any tile width).
+bool plan_for_length(int F, FftPlan *p);
+int variant_for_plan(const FftPlan &p, int need_nl);
+
 void note_launch();
 
 }  // namespace vfd

@@ -138,6 +138,20 @@ static int pick_variant(const std::vector<FftPlan> &plans, int need_nl = 0)
     return -1;
 }
 
+// Plan and kernel-variant lookup without heap use, for the allocation-free
+// entry point (vfd_noalloc.cu); same radices and variant preference as above.
+bool plan_for_length(int F, FftPlan *p) { return make_plan(F, p) && any_variant_fits(*p); }
+
+int variant_for_plan(const FftPlan &p, int need_nl)
+{
+    static const int pref[] = {2, 3, 1, 0, 5, 4};
+    for (int v : pref) {
+        if (need_nl && kAxisVariants[v].nl != need_nl) continue;
+        if (variant_fits(v, p)) return v;
+    }
+    return -1;
+}
+
 // Real multipliers G(k)/F of the wrapped normalised Gaussian taps, FP64.
 static void gauss_spectrum(double sigma, int r, int F, std::vector<float> &out)
 {

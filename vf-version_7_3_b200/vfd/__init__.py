@@ -43,6 +43,7 @@ EXPORTED = [
     "vfd_set_window", "vfd_synth_field_device", "vfd_stencil_window",
     "vfd_server_create", "vfd_server_submit", "vfd_server_wait", "vfd_server_drain",
     "vfd_server_get_stats", "vfd_server_clock", "vfd_server_destroy",
+    "vfd_fft_diffuse3d_noalloc",
 ]
 
 
@@ -126,6 +127,7 @@ def load(path=LIB_PATH):
     lib.vfd_batch_destroy.argtypes = [P]
     lib.vfd_batch_last_error.argtypes = [P]
     lib.vfd_batch_last_error.restype = C.c_char_p
+    lib.vfd_fft_diffuse3d_noalloc.argtypes = [P, P] + [C.c_int] * 8 + [C.c_float] * 3 + [P]
     lib.vfd_stencil_window.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, P, C.c_int]
     lib.vfd_synth_field_device.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_float, C.c_float, P,
                                            C.c_size_t, P]
