@@ -362,6 +362,7 @@ def main():
     ap.add_argument("--cpu-fields", type=int, default=2,
                     help="fields in the CPU-baseline sample (1 substep each)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain per-field path timing")
     args = ap.parse_args()
     if args.config == "cfg2" and args.impl == "vfd":
         run_cfg2(args)
@@ -429,12 +430,10 @@ def main():
     ms = e0.elapsed_time(e1)
     prof = world.read_profile()
     world.set_profiling(False)
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    from vfd import dist as vd
+    ms = vd.max_over_ranks(ms, device=f"cuda:{dev}")
     vsteps = V * nf * c["substeps"] * args.steps
-    value = ws * vsteps / (ms / 1e3)
+    value = vd.aggregate_rate(vsteps, ms / 1e3, ws)
 
     # roofline of the dominant kernel (axis pass): 8 B per voxel per field per launch
     axis_ms = sum(prof[k][0] for k in ("x", "y", "z"))
@@ -468,15 +467,31 @@ def main():
             world.set_sources(f, idx, amt)
         world.diffuse_host(host_in, host_out, c["substeps"])
     t_e2e = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([t_e2e], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = vd.max_over_ranks(t_e2e, device=f"cuda:{dev}")
     e2e = {"value": ws * V * nf * c["substeps"] * args.e2e_steps / t_e2e, "unit": METRIC,
            "h2d_bytes_per_step": nf * V * 4 + sum(i.nbytes + a.nbytes for _, i, a in ins),
            "d2h_bytes_per_step": nf * V * 4,
            "api": "vfd_diffuse_host (pinned host buffers in and out, the diffuseChemGPU contract)",
            "steps": args.e2e_steps}
+
+    # the plain per-field path on the same world (unfused kernels in the
+    # reference's order, one field after another, no graph): one tick
+    plain = None
+    if not args.no_plain and ws == 1:
+        pw = vfd.World(nx, ny, nz, params, device=dev, method=vfd.METHOD_PLAIN)
+        for f, (u, idx, amt) in enumerate(ins):
+            pw.upload(f, u)
+            pw.set_sources(f, idx, amt)
+        pw.tick(1, stream=sh)
+        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        q0.record(stream)
+        pw.tick(c["substeps"], stream=sh)
+        q1.record(stream)
+        torch.cuda.synchronize(dev)
+        plain = {"value": V * nf * c["substeps"] / (q0.elapsed_time(q1) / 1e3), "unit": METRIC,
+                 "what": "VFD_METHOD_PLAIN: pad, R2C, C2C y, C2C z, multiply, C2C z, C2C y, C2R, crop as "
+                         "separate kernels per field, no graph (1 tick)"}
+        pw.close()
 
     line = None
     if rank == 0:
@@ -489,7 +504,8 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic (seeded counter-based generator)",
                 "config": workload_config(c, world.fft_dims()), "roofline": roofline,
-                "cpu_baseline": cb, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+                "cpu_baseline": cb, "e2e": e2e, "plain_gpu": plain, "gpu_launches": launches,
+                "clocks": clk}
     world.close()
     if dist is not None:
         dist.barrier()

@@ -99,3 +99,86 @@ done:
     cudaFree(d_ds);
     return rc;
 }
+
+// Times the reference's per-field diffusion on the device, window spectrum
+// prepared once.  ms[0]: the kernels + cuFFT of one fftDiffuse3D call
+// (memset, padDataConstantVF3D, R2C, modulateAndNormalize3D, C2R,
+// unpadResult3D) with buffers and plans reused; ms[1]: the same call as the
+// reference makes it each tick -- cufftPlan3d x2 (Diffuser.cpp:273-274),
+// cudaMalloc of the padded and spectrum buffers (Diffusion.cu:1686-1687),
+// the kernels, cudaFree and cufftDestroy.  Averages over `iters` calls.
+extern "C" int ref_replay_time(int D, int H, int W, int fftD, int fftH, int fftW, const float *h_win, int kD,
+                               int kH, int kW, int kZ, int kY, int kX, int epi, float baseChem, int iters,
+                               double *ms)
+{
+    int rc = 0;
+    float *d_data = nullptr, *d_win = nullptr, *d_pk = nullptr, *d_pad = nullptr;
+    float2 *d_ks = nullptr, *d_ds = nullptr;
+    cufftHandle fwd = 0, inv = 0;
+    bool have_fwd = false, have_inv = false;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const size_t dsz = (size_t)D * H * W, fsz = (size_t)fftD * fftH * fftW;
+    const size_t ssz = (size_t)fftD * fftH * (fftW / 2 + 1);
+    const size_t wsz = (size_t)kD * kH * kW;
+    float t = 0.0f;
+    RR_CHECK(cudaEventCreate(&e0));
+    RR_CHECK(cudaEventCreate(&e1));
+    RR_CHECK(cudaMalloc(&d_data, dsz * sizeof(float)));
+    RR_CHECK(cudaMemset(d_data, 0, dsz * sizeof(float)));
+    RR_CHECK(cudaMalloc(&d_win, wsz * sizeof(float)));
+    RR_CHECK(cudaMalloc(&d_pk, fsz * sizeof(float)));
+    RR_CHECK(cudaMalloc(&d_ks, ssz * sizeof(float2)));
+    RR_CHECK(cudaMemcpy(d_win, h_win, wsz * sizeof(float), cudaMemcpyHostToDevice));
+    RR_CUFFT(cufftPlan3d(&fwd, fftD, fftH, fftW, CUFFT_R2C));
+    have_fwd = true;
+    RR_CUFFT(cufftPlan3d(&inv, fftD, fftH, fftW, CUFFT_C2R));
+    have_inv = true;
+    RR_CHECK(cudaMemset(d_pk, 0, fsz * sizeof(float)));
+    padKernel3D(d_pk, d_win, fftD, fftH, fftW, kD, kH, kW, kZ, kY, kX);
+    RR_CUFFT(cufftExecR2C(fwd, (cufftReal *)d_pk, (cufftComplex *)d_ks));
+    RR_CHECK(cudaMalloc(&d_pad, fsz * sizeof(float)));
+    RR_CHECK(cudaMalloc(&d_ds, ssz * sizeof(float2)));
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int it = -1; it < iters; ++it) {  // it = -1: warm-up
+            if (it == 0) RR_CHECK(cudaEventRecord(e0));
+            cufftHandle f2 = fwd, i2 = inv;
+            float *pad = d_pad;
+            float2 *ds = d_ds;
+            if (pass == 1) {
+                RR_CUFFT(cufftPlan3d(&f2, fftD, fftH, fftW, CUFFT_R2C));
+                RR_CUFFT(cufftPlan3d(&i2, fftD, fftH, fftW, CUFFT_C2R));
+                RR_CHECK(cudaMalloc(&pad, fsz * sizeof(float)));
+                RR_CHECK(cudaMalloc(&ds, ssz * sizeof(float2)));
+            }
+            RR_CHECK(cudaMemset(pad, 0, fsz * sizeof(float)));
+            padDataConstantVF3D(pad, d_data, fftD, fftH, fftW, D, H, W, kD, kH, kW, kZ, kY, kX, epi, baseChem);
+            RR_CUFFT(cufftExecR2C(f2, (cufftReal *)pad, (cufftComplex *)ds));
+            modulateAndNormalize3D(ds, d_ks, fftD, fftH, fftW, 1);
+            RR_CUFFT(cufftExecC2R(i2, (cufftComplex *)ds, (cufftReal *)pad));
+            unpadResult3D(d_data, pad, D, H, W, fftD, fftH, fftW);
+            if (pass == 1) {
+                RR_CHECK(cudaDeviceSynchronize());
+                cudaFree(pad);
+                cudaFree(ds);
+                cufftDestroy(f2);
+                cufftDestroy(i2);
+            }
+        }
+        RR_CHECK(cudaEventRecord(e1));
+        RR_CHECK(cudaEventSynchronize(e1));
+        RR_CHECK(cudaEventElapsedTime(&t, e0, e1));
+        ms[pass] = (double)t / iters;
+    }
+done:
+    if (have_fwd) cufftDestroy(fwd);
+    if (have_inv) cufftDestroy(inv);
+    cudaFree(d_data);
+    cudaFree(d_win);
+    cudaFree(d_pk);
+    cudaFree(d_pad);
+    cudaFree(d_ks);
+    cudaFree(d_ds);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    return rc;
+}

@@ -234,3 +234,22 @@ def test_wide_kernel_uses_full_line_path(gpu, sigma):
     ref = oracle.tick(u, sigma, 0.03, 2, idx, amt)
     assert rel_l2(outs[0], ref) <= REL_L2
     check_mass(outs[0], mass[0], 0.97, 0.0, nx * ny * nz)
+
+
+def test_cfg4_large_world_one_field_against_oracle(gpu):
+    """Large-world stress grid (768x384x576, padding limited to the kernel
+    support) at full size: the widest-kernel field (sigma 2.6, radius 8),
+    10 substeps, 1M sources, against the FP64 oracle."""
+    c = configs.CFG4
+    nx, ny, nz = c["grid"]
+    f = 6
+    u = vfd.synth_field(c["seed"], 0, f, (nz, ny, nx))
+    idx, amt = vfd.synth_sources(c["seed"], 0, f, c["n_sources"], nx * ny * nz)
+    outs, mass, dims = run_world(c["grid"], [c["sigma"][f]], [c["decay"][f]], [(u, idx, amt)],
+                                 substeps=c["substeps"])
+    del u
+    ref = oracle.tick(vfd.synth_field(c["seed"], 0, f, (nz, ny, nx)), c["sigma"][f], c["decay"][f],
+                      c["substeps"], idx, amt)
+    e = rel_l2(outs[0], ref)
+    assert e <= REL_L2, e
+    check_mass(outs[0], mass[0], 1 - c["decay"][f], 0.0, nx * ny * nz)

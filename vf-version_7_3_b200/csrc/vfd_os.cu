@@ -332,6 +332,221 @@ __global__ void __launch_bounds__(OS_NT, MINB) os_pass_kernel(const OsJob *__res
     }
 }
 
+// ---------------------------------------------------------------------------
+// Pipelined variant: the next chunk's new input positions are fetched with
+// cp.async (4-byte, zero-filled outside the line) into the second of two
+// staging buffers while the current chunk's FFTs run.  Used when staging
+// needs no transform on load (zero padding: v = u); the input mass of the x
+// pass is summed from the samples that are block outputs (each staged
+// position inside the chunk's output range exactly once).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async4(float *smem, const float *gmem, bool valid)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? 4 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Issues the asynchronous staging of positions [ifirst, NP) of chunk (p0) into
+// stage (float view).  Rows/columns beyond nreal and positions outside
+// [0, n) are zero-filled.
+__device__ __forceinline__ void os_stage_async(float *stage, const OsJob &j, float *base, int nreal, int p0,
+                                               int ifirst, int NP)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int NW = OS_NT / 32;
+    const int n = j.n;
+    if (j.kind == PASS_X) {
+        for (int row = warp; row < 32; row += NW) {
+            const bool ok = row < nreal;
+            const float *src = base + (int64_t)(ok ? row : 0) * j.line_stride;
+            float *dst = stage + 2 * (row & 15) + (row >> 4);
+            for (int i = ifirst + lane; i < NP; i += 32) {
+                const int p = p0 + i;
+                const bool v = ok && p >= 0 && p < n;
+                cp_async4(dst + i * 2 * OS_LS, v ? src + p : src, v);
+            }
+        }
+    } else {
+        const int64_t ps = j.pos_stride;
+        const bool ok = lane < nreal;
+        const float *src = base + (int64_t)(ok ? lane : 0) * j.line_stride;
+        float *dst = stage + 2 * (lane & 15) + (lane >> 4);
+        for (int i = ifirst + warp; i < NP; i += NW) {
+            const int p = p0 + i;
+            const bool v = ok && p >= 0 && p < n;
+            cp_async4(dst + i * 2 * OS_LS, v ? src + (int64_t)p * ps : src, v);
+        }
+    }
+}
+
+template <int M, int MINB>
+__global__ void __launch_bounds__(OS_NT, MINB) os_pass_pipe_kernel(const OsJob *__restrict__ jobs, int njobs)
+{
+    extern __shared__ __align__(16) float2 osm[];
+    __shared__ double red[OS_NT / 32];
+    __shared__ OsJob sj;
+    __shared__ float2 tw64[64];
+
+    const int tile = blockIdx.x;
+    if (threadIdx.x == 0) {
+        int lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (jobs[mid].tile_begin <= tile) lo = mid;
+            else hi = mid - 1;
+        }
+        sj = jobs[lo];
+    }
+    if (threadIdx.x < 64) {
+        double sn, cs;
+        sincospi((double)threadIdx.x / 32.0, &sn, &cs);
+        tw64[threadIdx.x] = make_float2((float)cs, (float)-sn);
+    }
+    __syncthreads();
+
+    const int n = sj.n, r = sj.r, L = sj.L, C = sj.C;
+    const int NP = C + 2 * r;
+    // two staging buffers [NP][OS_LS] at osm and osm + NP * OS_LS
+    float2 *out = osm + 2 * NP * OS_LS;        // [C][OS_LS]
+    float2 *scr = out + C * OS_LS;             // [32 groups][OS_SCR]
+    float *outf = reinterpret_cast<float *>(out);
+
+    const int local = tile - sj.tile_begin;
+    const int outer = local / sj.tiles_per_outer;
+    const int lt = local - outer * sj.tiles_per_outer;
+    const int l0 = lt * 32;
+    const int nreal = min(32, sj.nlines - l0);
+    float *base = sj.data + outer * sj.outer_stride + (int64_t)l0 * sj.line_stride;
+    const int kind = sj.kind;
+    const float b = sj.b;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int NW = OS_NT / 32;
+
+    const int g = threadIdx.x >> 3, t = threadIdx.x & 7;
+    float2 *gs = scr + g * OS_SCR;
+    float2 w[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) w[k] = tw64[(t * k) & 63];
+    unsigned qmask = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int i = t + 8 * q;
+        if (i >= r && i < r + L) qmask |= 1u << q;
+    }
+    const int64_t ps = sj.pos_stride;
+    const int nch = sj.nchunks;
+
+    os_stage_async(reinterpret_cast<float *>(osm), sj, base, nreal, -2 * r, 0, NP);
+    cp_async_commit();
+
+    double acc_in = 0.0, acc_leak = 0.0, acc_conv = 0.0, acc_out = 0.0;
+    for (int ch = 0; ch < nch; ++ch) {
+        const int c0 = -r + ch * C, p0 = c0 - r;
+        float2 *in = osm + (ch & 1) * NP * OS_LS;
+        float2 *nxt = osm + ((ch & 1) ^ 1) * NP * OS_LS;
+        // this chunk's samples have landed; every thread has also finished the
+        // previous iteration (its halo copy out of `nxt` and its reads of `out`)
+        cp_async_wait<0>();
+        __syncthreads();
+        if (ch + 1 < nch) {
+            // next chunk: positions [2r, NP) from global memory (not yet
+            // overwritten: this chunk stores only outputs below p0 + C + 2r)
+            os_stage_async(reinterpret_cast<float *>(nxt), sj, base, nreal, p0 + C, 2 * r, NP);
+            cp_async_commit();
+        }
+
+        const bool out_inside = c0 >= 0 && c0 + C <= n;
+        for (int u = g; u < OS_PAIRS * M; u += OS_NT / 8) {
+            const int pair = ((u & 1) << 3) | ((u >> 1) & 7);
+            const int seg0 = (u >> 4) * L;
+            const float2 *sp = in + (seg0 + t) * OS_LS + pair;
+            float2 x[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) x[q] = sp[q * 8 * OS_LS];
+            if (kind == PASS_X) {
+                // input mass: the samples this block outputs (own positions)
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if ((qmask >> q) & 1u) acc_in += (double)x[q].x + (double)x[q].y;
+            }
+            fft64_fwd(x, t, gs, w);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const float h = sj.H[t + 8 * k];
+                x[k] = make_float2(x[k].x * h, x[k].y * h);
+            }
+            fft64_inv(x, t, gs, w);
+            float2 *op = out + (seg0 + t - r) * OS_LS + pair;
+            if (out_inside) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if ((qmask >> q) & 1u) op[q * 8 * OS_LS] = x[q];
+            } else {
+                const int o0 = c0 + seg0 + t - r;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    if ((qmask >> q) & 1u) {
+                        const int o = o0 + 8 * q;
+                        if (o >= 0 && o < n) op[q * 8 * OS_LS] = x[q];
+                        else acc_leak += (double)x[q].x + (double)x[q].y;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // carry the next chunk's first 2r positions (disjoint from its async part)
+        if (ch + 1 < nch)
+            for (int i = threadIdx.x; i < 2 * r * OS_LS; i += OS_NT) nxt[i] = in[C * OS_LS + i];
+
+        const int jlo = max(0, -c0), jhi = min(C, n - c0);
+        if (kind == PASS_X) {
+            for (int row = warp; row < nreal; row += NW) {
+                float *dst = base + (int64_t)row * sj.line_stride + c0;
+                const float *sv = outf + 2 * (row & 15) + (row >> 4);
+                for (int j = jlo + lane; j < jhi; j += 32) dst[j] = sv[j * 2 * OS_LS];
+            }
+        } else if (lane < nreal) {
+            const float *sv = outf + (jlo + warp) * 2 * OS_LS + 2 * (lane & 15) + (lane >> 4);
+            float *dst = base + (int64_t)lane * sj.line_stride + (int64_t)(c0 + jlo + warp) * ps;
+            const int64_t step = (int64_t)NW * ps;
+            if (kind == PASS_Z) {
+                const float keep = sj.keep;
+                for (int j = jlo + warp; j < jhi; j += NW) {
+                    float v = *sv;
+                    acc_conv += (double)v;
+                    v = keep * (v + b);
+                    acc_out += (double)v;
+                    *dst = v;
+                    sv += NW * 2 * OS_LS;
+                    dst += step;
+                }
+            } else {
+                for (int j = jlo + warp; j < jhi; j += NW) {
+                    *dst = *sv;
+                    sv += NW * 2 * OS_LS;
+                    dst += step;
+                }
+            }
+        }
+    }
+
+    double *mass = sj.mass;
+    if (kind == PASS_X) {
+        os_block_sum(acc_in, mass + MS_INPUT, red);
+        os_block_sum(acc_leak, mass + MS_LEAK_X, red);
+    } else if (kind == PASS_Y) {
+        os_block_sum(acc_leak, mass + MS_LEAK_Y, red);
+    } else {
+        os_block_sum(acc_leak, mass + MS_LEAK_Z, red);
+        os_block_sum(acc_conv, mass + MS_CONV, red);
+        os_block_sum(acc_out, mass + MS_OUT, red);
+    }
+}
+
 int os_blocks_per_chunk()
 {
     static int m = -1;
@@ -365,10 +580,63 @@ static cudaError_t launch_os_t(const OsJob *jobs, int njobs, int tiles, int rmin
     return cudaGetLastError();
 }
 
+static int os_min_blocks()
+{
+    static int m = -1;
+    if (m < 0) {
+        const char *e = getenv("VFD_OS_MINB");
+        m = (e && e[0] == '3') ? 3 : 4;  // 4 blocks per SM (64 registers) measured faster on B200
+    }
+    return m;
+}
+
+size_t os_pipe_smem_bytes(int rmin, int M)
+{
+    const int L = OS_N - 2 * rmin, C = M * L;
+    return ((size_t)2 * (C + 2 * rmin) * OS_LS + (size_t)C * OS_LS + (size_t)(OS_NT / 8) * OS_SCR) *
+           sizeof(float2);
+}
+
+template <int M, int MINB>
+static cudaError_t launch_os_pipe_t(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st)
+{
+    static thread_local int configured_dev = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured_dev != dev) {
+        cudaError_t e = cudaFuncSetAttribute(os_pass_pipe_kernel<M, MINB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axis_smem_limit());
+        if (e != cudaSuccess) return e;
+        configured_dev = dev;
+    }
+    os_pass_pipe_kernel<M, MINB><<<tiles, OS_NT, os_pipe_smem_bytes(rmin, M), st>>>(jobs, njobs);
+    note_launch();
+    return cudaGetLastError();
+}
+
+bool os_pipe_enabled()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("VFD_OS_PIPE");
+        on = (e && e[0] == '0') ? 0 : 1;
+    }
+    return on == 1;
+}
+
+cudaError_t launch_os_pipe(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st)
+{
+    if (tiles <= 0) return cudaSuccess;
+    if (os_blocks_per_chunk() == 4) return launch_os_pipe_t<4, 2>(jobs, njobs, tiles, rmin, st);
+    if (os_min_blocks() == 4) return launch_os_pipe_t<2, 4>(jobs, njobs, tiles, rmin, st);
+    return launch_os_pipe_t<2, 3>(jobs, njobs, tiles, rmin, st);
+}
+
 cudaError_t launch_os(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st)
 {
     if (tiles <= 0) return cudaSuccess;
     if (os_blocks_per_chunk() == 4) return launch_os_t<4, 2>(jobs, njobs, tiles, rmin, st);
+    if (os_min_blocks() == 4) return launch_os_t<2, 4>(jobs, njobs, tiles, rmin, st);
     return launch_os_t<2, 3>(jobs, njobs, tiles, rmin, st);
 }
 

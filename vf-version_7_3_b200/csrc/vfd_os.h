@@ -33,5 +33,9 @@ struct OsJob {
 int os_blocks_per_chunk();
 size_t os_smem_bytes(int rmin, int M);
 cudaError_t launch_os(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st);
+// Pipelined variant for jobs whose staging needs no transform (zero padding);
+// VFD_OS_PIPE=0 disables it.
+bool os_pipe_enabled();
+cudaError_t launch_os_pipe(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st);
 
 }  // namespace vfd

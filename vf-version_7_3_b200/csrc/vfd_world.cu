@@ -200,6 +200,7 @@ struct vfd_world {
     int tiles_per_field[3] = {0, 0, 0};
     // overlap-save passes (kernel radius <= OS_RMAX): per axis
     bool use_os[3] = {false, false, false};
+    bool os_pipe[3] = {false, false, false};  // staging needs no transform: pipelined kernel
     int rmin[3] = {0, 0, 0};
     OsJob *d_osjobs = nullptr;             // [pass][nf] all-field, then [pass][nf] single-field
     std::vector<int> os_tiles[3];          // per field
@@ -406,6 +407,14 @@ static OsJob make_os_job(const vfd_world *w, int f, int a, int tile_begin)
 
 static int os_field_tiles(const OsJob &j) { return j.nouter * j.tiles_per_outer; }
 
+// True when the pass stages samples unchanged (no padding-rule transform).
+static bool os_plain_staging(const OsJob &j)
+{
+    if (j.kind != PASS_X) return true;
+    return j.b == 0.0f && j.box_lo[0] == 0 && j.box_hi[0] == j.nx && j.box_lo[1] == 0 && j.box_hi[1] == j.ny &&
+           j.box_lo[2] == 0 && j.box_hi[2] == j.nlines / j.ny;
+}
+
 extern "C" {
 
 const char *vfd_status_string(vfd_status s)
@@ -587,9 +596,11 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
         for (int a = 0; a < 3; ++a) {
             int tb = 0;
             w->os_tiles[a].assign(w->nf, 0);
+            w->os_pipe[a] = os_pipe_enabled();
             for (int f = 0; f < w->nf; ++f) {
                 oj.push_back(make_os_job(w, f, a, tb));
                 w->os_tiles[a][f] = os_field_tiles(oj.back());
+                w->os_pipe[a] = w->os_pipe[a] && os_plain_staging(oj.back());
                 tb += w->os_tiles[a][f];
             }
         }
@@ -1054,7 +1065,8 @@ static vfd_status enqueue_tick(vfd_world *w, int field, int n_substeps, cudaStre
                     for (int f = 0; f < w->nf; ++f) tiles += w->os_tiles[a][f];
                 else
                     tiles = w->os_tiles[a][field];
-                VFD_CUDA(w, launch_os(jobs, nj, tiles, w->rmin[a], st));
+                if (w->os_pipe[a]) VFD_CUDA(w, launch_os_pipe(jobs, nj, tiles, w->rmin[a], st));
+                else VFD_CUDA(w, launch_os(jobs, nj, tiles, w->rmin[a], st));
             } else {
                 const AxisJob *jobs = field < 0 ? w->d_jobs + a * w->nf : w->d_jobs + 3 * w->nf + a * w->nf + field;
                 const int tiles = w->tiles_per_field[a] * nj;
@@ -1197,6 +1209,7 @@ struct vfd_batch {
     int njobs = 0;
     AxisJob *d_jobs = nullptr;  // [3][njobs]
     bool use_os[3] = {false, false, false};
+    bool os_pipe[3] = {false, false, false};
     int rmin[3] = {0, 0, 0};
     OsJob *d_osjobs = nullptr;  // [3][njobs]
     int os_tiles[3] = {0, 0, 0};
@@ -1296,9 +1309,11 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
     if (b->use_os[0] || b->use_os[1] || b->use_os[2]) {
         for (int a = 0; a < 3; ++a) {
             int tb = 0;
+            b->os_pipe[a] = os_pipe_enabled();
             for (auto *w : b->worlds)
                 for (int f = 0; f < w->nf; ++f) {
                     oj.push_back(make_os_job(w, f, a, tb));
+                    b->os_pipe[a] = b->os_pipe[a] && os_plain_staging(oj.back());
                     tb += os_field_tiles(oj.back());
                 }
             b->os_tiles[a] = tb;
@@ -1345,7 +1360,10 @@ static vfd_status batch_enqueue(vfd_batch *b, int n_substeps)
         for (auto *w : b->worlds)
             VFD_BCUDA(b, cudaMemsetAsync(w->d_mass, 0, sizeof(double) * MS_COUNT * w->nf, b->st));
         for (int a = 0; a < 3; ++a) {
-            if (b->use_os[a])
+            if (b->use_os[a] && b->os_pipe[a])
+                VFD_BCUDA(b, launch_os_pipe(b->d_osjobs + a * b->njobs, b->njobs, b->os_tiles[a], b->rmin[a],
+                                            b->st));
+            else if (b->use_os[a])
                 VFD_BCUDA(b, launch_os(b->d_osjobs + a * b->njobs, b->njobs, b->os_tiles[a], b->rmin[a], b->st));
             else
                 VFD_BCUDA(b, launch_axis(b->variant[a], b->d_jobs + a * b->njobs, b->njobs, b->tiles[a],
