@@ -282,6 +282,26 @@ vfd_status vfd_fft_diffuse3d_noalloc(float *field, const float *kspec, int nx, i
 vfd_status vfd_world_set_profiling(vfd_world *w, int enable);
 vfd_status vfd_read_profile(vfd_world *w, double *ms4, int64_t *launches4);
 
+/* ---- steps either side of the diffusion -----------------------------------
+ * Attractant gradients of WHChemical::update (WHChemical.cpp:433-441) from a
+ * world whose fields are in the reference's chemical order (TNF, TGF, FGF,
+ * MMP8, IL1, IL6, IL8, IL10; src/enums.h:124-138):
+ *   grad = IL1 + TNF + TGF + FGF + collagen;  fib = TGF;
+ *   neu = grad + IL6 + IL8;  mac = grad + elastin.
+ * All pointers are device arrays of nx*ny*nz floats; collagen / elastin
+ * (the ECM fragment counts) may be NULL (zero); any output may be NULL. */
+vfd_status vfd_update_gradients(vfd_world *w, const float *collagen, const float *elastin,
+                                float *fib, float *neu, float *mac, void *stream);
+/* The compute part of sampleChem (volumeRender_kernel.cu:215-321): out
+ * (device, (nx/stride)*(ny/stride)*(nz/stride) floats, x fastest) receives
+ * min(field[stride*dx, stride*dy, stride*dz] * scale, 1).  The reference uses
+ * stride 3 and scales 5e4, 1e4, 1e6, 100, 1e4, 1e5, 1e5, 1e4 per chemical. */
+vfd_status vfd_sample_field(vfd_world *w, int field, int stride, float scale, float *out, void *stream);
+/* Legacy-VTK ASCII STRUCTURED_POINTS file of one host field (scalars
+ * "Color", x fastest, one line per row: the layout of util::outputChem,
+ * output_utils.h:813-854), values with 9 significant digits. */
+vfd_status vfd_write_vtk(const float *field, int nx, int ny, int nz, const char *path);
+
 /* ---- diagnostics ------------------------------------------------------ */
 const char *vfd_status_string(vfd_status s);
 /* Last error message of this world (or of the last failed create when

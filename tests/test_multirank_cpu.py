@@ -39,7 +39,7 @@ def _worker(rank, ws, port, out):
 def test_two_rank_plumbing():
     ws = 2
     port = _free_port()
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.spawn(_worker, args=(ws, port, out), nprocs=ws, join=True)
         res = dict(out)

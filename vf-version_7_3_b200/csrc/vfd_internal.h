@@ -55,6 +55,11 @@ cudaError_t launch_synth_field(uint64_t key, double lo, double span, float *out,
 bool plan_for_length(int F, FftPlan *p);
 int variant_for_plan(const FftPlan &p, int need_nl);
 
+cudaError_t launch_gradients(const float *const *chem, const float *col, const float *ela, float *fib, float *neu,
+                             float *mac, int64_t n, cudaStream_t st);
+cudaError_t launch_sample(const float *src, int nx, int ny, int nz, int stride, float scale, float *out,
+                          cudaStream_t st);
+
 void note_launch();
 
 }  // namespace vfd

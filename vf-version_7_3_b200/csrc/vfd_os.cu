@@ -627,8 +627,8 @@ bool os_pipe_enabled()
 cudaError_t launch_os_pipe(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st)
 {
     if (tiles <= 0) return cudaSuccess;
+    // the pipelined kernel measured fastest at 3 blocks per SM (80 registers)
     if (os_blocks_per_chunk() == 4) return launch_os_pipe_t<4, 2>(jobs, njobs, tiles, rmin, st);
-    if (os_min_blocks() == 4) return launch_os_pipe_t<2, 4>(jobs, njobs, tiles, rmin, st);
     return launch_os_pipe_t<2, 3>(jobs, njobs, tiles, rmin, st);
 }
 

@@ -1135,6 +1135,29 @@ vfd_status vfd_read_mass(vfd_world *w, vfd_mass *out, void *stream)
     return VFD_OK;
 }
 
+vfd_status vfd_update_gradients(vfd_world *w, const float *collagen, const float *elastin, float *fib, float *neu,
+                                float *mac, void *stream)
+{
+    if (!w) return VFD_ERR_INVALID_ARG;
+    if (w->nf < 7) return fail(w, VFD_ERR_INVALID_ARG, "gradients need the TNF..IL8 fields (n_fields >= 7)");
+    DeviceGuard g(w->device);
+    const float *chem[8];
+    for (int f = 0; f < 7; ++f) chem[f] = w->d_fields + (int64_t)f * w->V;
+    VFD_CUDA(w, launch_gradients(chem, collagen, elastin, fib, neu, mac, w->V, (cudaStream_t)stream));
+    return VFD_OK;
+}
+
+vfd_status vfd_sample_field(vfd_world *w, int field, int stride, float scale, float *out, void *stream)
+{
+    if (!w) return VFD_ERR_INVALID_ARG;
+    if (field < 0 || field >= w->nf || stride < 1 || !out)
+        return fail(w, VFD_ERR_INVALID_ARG, "bad field, stride or output pointer");
+    DeviceGuard g(w->device);
+    VFD_CUDA(w, launch_sample(w->d_fields + (int64_t)field * w->V, w->nx, w->ny, w->nz, stride, scale, out,
+                              (cudaStream_t)stream));
+    return VFD_OK;
+}
+
 vfd_status vfd_world_set_profiling(vfd_world *w, int enable)
 {
     if (!w) return VFD_ERR_INVALID_ARG;

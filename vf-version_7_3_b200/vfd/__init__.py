@@ -43,7 +43,7 @@ EXPORTED = [
     "vfd_set_window", "vfd_synth_field_device", "vfd_stencil_window",
     "vfd_server_create", "vfd_server_submit", "vfd_server_wait", "vfd_server_drain",
     "vfd_server_get_stats", "vfd_server_clock", "vfd_server_destroy",
-    "vfd_fft_diffuse3d_noalloc",
+    "vfd_fft_diffuse3d_noalloc", "vfd_update_gradients", "vfd_sample_field", "vfd_write_vtk",
 ]
 
 
@@ -128,6 +128,9 @@ def load(path=LIB_PATH):
     lib.vfd_batch_last_error.argtypes = [P]
     lib.vfd_batch_last_error.restype = C.c_char_p
     lib.vfd_fft_diffuse3d_noalloc.argtypes = [P, P] + [C.c_int] * 8 + [C.c_float] * 3 + [P]
+    lib.vfd_update_gradients.argtypes = [P, P, P, P, P, P, P]
+    lib.vfd_sample_field.argtypes = [P, C.c_int, C.c_int, C.c_float, P, P]
+    lib.vfd_write_vtk.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_char_p]
     lib.vfd_stencil_window.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, P, C.c_int]
     lib.vfd_synth_field_device.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_float, C.c_float, P,
                                            C.c_size_t, P]
@@ -296,6 +299,14 @@ class World:
         _check(lib().vfd_read_mass(self._h, m, stream), self._h)
         return [x.as_dict() for x in m]
 
+    def update_gradients(self, collagen=0, elastin=0, fib=0, neu=0, mac=0, stream=None):
+        """Device pointers (ints, 0 = NULL) of nx*ny*nz float arrays."""
+        _check(lib().vfd_update_gradients(self._h, collagen or None, elastin or None, fib or None,
+                                          neu or None, mac or None, stream), self._h)
+
+    def sample(self, field, stride, scale, out_ptr, stream=None):
+        _check(lib().vfd_sample_field(self._h, field, stride, scale, out_ptr, stream), self._h)
+
     def set_profiling(self, enable=True):
         _check(lib().vfd_world_set_profiling(self._h, int(bool(enable))), self._h)
 
@@ -351,6 +362,13 @@ class Batch:
 
     def __exit__(self, *a):
         self.close()
+
+
+def write_vtk(field, path):
+    """Legacy-VTK ASCII file of a (nz, ny, nx) float32 field."""
+    a = np.ascontiguousarray(field, np.float32)
+    nz, ny, nx = a.shape
+    _check(lib().vfd_write_vtk(_ptr(a), nx, ny, nz, str(path).encode()))
 
 
 def stencil_window(lam, gamma_dt, n_steps, R, device=0):
