@@ -9,38 +9,61 @@
 // forward FFT-64, multiply by the kernel's 64-point spectrum, inverse
 // FFT-64, keep L samples -- the reference's pad / R2C / modulate / C2R / crop
 // (Diffusion.cu:1731-1859) applied per block.  Blocks cover output positions
-// [-r, n + r); outputs outside [0, n) are the mass pushed past the crop and
-// are summed as the leak instead of being stored.
+// [ofirst, n + r) with ofirst <= -r; outputs in [-r, 0) and [n, n + r) are
+// the mass pushed past the crop and are summed as the leak instead of being
+// stored (outputs further out are zero: no input reaches them).
 //
-// Work split: a CTA owns 32 real lines (16 complex pairs: line q is the real
-// part of pair q % 16 for q < 16, the imaginary part otherwise -- the kernel
-// spectrum is real and even, so the pair's parts are convolved independently)
-// over their whole length, processed in chunks of M consecutive blocks.  The
-// field is updated in place: a chunk's 2r-sample input halo that overlaps
-// the previous chunk's outputs is carried forward in shared memory before
-// those outputs are stored, so no CTA ever reads a sample another chunk has
-// already overwritten (and no two CTAs share a line).  A group of 8 lanes
-// computes one (pair, block) FFT: lane t holds samples t + 8q (q = 0..7);
+// Work split: a CTA owns 32 real lines of one outer index over their whole
+// length, processed in chunks of 2 blocks (C = 2L outputs).  Lines 2p and
+// 2p+1 form complex pair p (real and imaginary part): the kernel spectrum is
+// real and even, so one complex FFT convolves both independently.  A group
+// of 8 lanes computes one (pair, block) FFT; the 32 groups of a CTA cover
+// the 16 pairs x 2 blocks of a chunk.
+//
+// Pipeline and in-place update: while chunk ch is transformed, chunk ch+1's
+// input (its whole window, halo included) is fetched with cp.async into the
+// second staging buffer; every thread waits for those copies and the CTA
+// synchronises before chunk ch's outputs are stored.  So no sample is read
+// after a chunk of the same lines overwrote it, and no two CTAs share a line.
+//
+// Staging layouts (what keeps a voxel's cost close to its FFT's):
+//   * y/z passes stage position rows of 36 floats (32 lines + 4 pad, 144
+//     bytes): one 16-byte cp.async moves 4 lines of one position, one
+//     16-byte store writes 4 lines back (the lines are contiguous in x);
+//   * the x pass stages line rows (positions contiguous) from a window that
+//     starts on a 16-byte boundary, `delta` positions before the chunk's
+//     first input, and its chunks start on multiples of 4 (ofirst), so both
+//     the copies in and the stores out move 16 bytes along x;
+//   * line-row strides are = 4 (mod 16) floats, so the 4 groups of a warp
+//     (consecutive pairs, one block) touch disjoint bank octets;
+//   * the constant-VF padding rule of the x pass is applied in registers as
+//     samples enter the FFT.
+//
+// FFT-64 of one pair, by a group of 8 lanes: lane t holds samples t + 8q;
 //   forward : DFT-8 over q in registers, twiddle w64^(t k1), transpose
 //             through a swizzled per-group scratch (__syncwarp only), DFT-8
-//             over t;  lane k1 then holds bins k1 + 8 k2 (k2 = 0..7)
+//             over t;  lane k1 then holds bins k1 + 8 k2
 //   multiply: by G64(k) / 64 (FP64-generated, stored FP32)
 //   inverse : the mirror steps, back to samples t + 8q.
-// Global <-> shared traffic uses the same interleaved [position][17] complex
-// staging as the full-line kernel (conflict-free for the group pattern used).
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdlib.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
 
 #include "vfd_internal.h"
 #include "vfd_os.h"
 
 namespace vfd {
 
-constexpr int OS_NT = 256;             // threads per CTA: 32 groups of 8 lanes
-constexpr int OS_PAIRS = 16;
-constexpr int OS_LS = OS_PAIRS + 1;    // float2 per staged position
-constexpr int OS_SCR = 64 + 8;         // float2 per group scratch (64 + pad)
+constexpr int OS_NT = 256;      // threads per CTA: 32 groups of 8 lanes
+constexpr int OS_SCR = 64 + 8;  // float2 per group scratch (64 + pad)
+constexpr int OS_RS = 36;       // y/z staging: floats per position row
+constexpr int OS_MINB = 3;      // CTAs per SM (80 registers per thread)
+
+__constant__ float2 c_tw64[64];  // exp(-2 pi i m / 64), FP64-generated on the host
 
 __device__ __forceinline__ double os_warp_sum(double v)
 {
@@ -65,6 +88,7 @@ __device__ __forceinline__ void os_block_sum(double v, double *dst, double *red)
 
 // Forward FFT-64 of the 8 samples x[q] = s[t + 8q] of lane t of a group;
 // on return lane t holds bins t + 8 k2 in x[k2].  scr: the group's scratch.
+// All 32 lanes of the warp call it together (__syncwarp).
 __device__ __forceinline__ void fft64_fwd(float2 (&x)[8], int t, float2 *scr, const float2 (&w)[8])
 {
     Dft<8, false>::run(x);
@@ -95,383 +119,233 @@ __device__ __forceinline__ void fft64_inv(float2 (&x)[8], int t, float2 *scr, co
     Dft<8, true>::run(x);
 }
 
-template <int M, int MINB>
-__global__ void __launch_bounds__(OS_NT, MINB) os_pass_kernel(const OsJob *__restrict__ jobs, int njobs)
-{
-    extern __shared__ __align__(16) float2 osm[];
-    __shared__ double red[OS_NT / 32];
-    __shared__ OsJob sj;
-    __shared__ float2 tw64[64];
-
-    const int tile = blockIdx.x;
-    if (threadIdx.x == 0) {
-        int lo = 0, hi = njobs - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (jobs[mid].tile_begin <= tile) lo = mid;
-            else hi = mid - 1;
-        }
-        sj = jobs[lo];
-    }
-    if (threadIdx.x < 64) {
-        double sn, cs;
-        sincospi((double)threadIdx.x / 32.0, &sn, &cs);
-        tw64[threadIdx.x] = make_float2((float)cs, (float)-sn);
-    }
-    __syncthreads();
-
-    const int n = sj.n, r = sj.r, L = sj.L, C = sj.C;
-    const int NP = C + 2 * r;                 // staged input positions per chunk
-    float2 *in = osm;                         // [NP][OS_LS]
-    float2 *out = in + NP * OS_LS;            // [C][OS_LS]
-    float2 *scr = out + C * OS_LS;            // [32 groups][OS_SCR]
-    float *inf = reinterpret_cast<float *>(in);
-    float *outf = reinterpret_cast<float *>(out);
-
-    // this CTA owns 32 lines of one outer index, whole length, all chunks
-    const int local = tile - sj.tile_begin;
-    const int outer = local / sj.tiles_per_outer;
-    const int lt = local - outer * sj.tiles_per_outer;
-    const int l0 = lt * 32;
-    const int nreal = min(32, sj.nlines - l0);
-    float *base = sj.data + outer * sj.outer_stride + (int64_t)l0 * sj.line_stride;
-    const int kind = sj.kind;
-    const float b = sj.b;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr int NW = OS_NT / 32;
-
-    // per-lane constants of the FFT phase
-    const int g = threadIdx.x >> 3, t = threadIdx.x & 7;
-    float2 *gs = scr + g * OS_SCR;
-    float2 w[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) w[k] = tw64[(t * k) & 63];
-    unsigned qmask = 0;  // samples t + 8q that are outputs of a block
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const int i = t + 8 * q;
-        if (i >= r && i < r + L) qmask |= 1u << q;
-    }
-
-    // x-pass row state (lane = position; rows = lines of the tile)
-    int xlo = 0, xhi = 0;
-    unsigned rowin_mask = 0;  // bit row: row inside the padding rule's y/z range
-    if (kind == PASS_X) {
-        xlo = sj.box_lo[0];
-        xhi = sj.box_hi[0];
-        for (int row = 0; row < nreal; ++row) {
-            const int rr = l0 + row;
-            const int y = rr % sj.ny, z = rr / sj.ny;
-            if (y >= sj.box_lo[1] && y < sj.box_hi[1] && z >= sj.box_lo[2] && z < sj.box_hi[2])
-                rowin_mask |= 1u << row;
-        }
-    }
-    const int64_t ps = sj.pos_stride;
-
-    double acc_in = 0.0, acc_leak = 0.0, acc_conv = 0.0, acc_out = 0.0;
-    for (int ch = 0; ch < sj.nchunks; ++ch) {
-        const int c0 = -r + ch * C;           // first output position of the chunk
-        const int p0 = c0 - r;                // first staged input position
-        // positions [p0, p0 + 2r) were staged by the previous chunk (its last
-        // 2r slots) before it overwrote anything; bring them forward and load
-        // only the rest from global memory
-        int ifirst = 0;
-        if (ch > 0) {
-            for (int i = threadIdx.x; i < 2 * r * OS_LS; i += OS_NT) in[i] = in[C * OS_LS + i];
-            ifirst = 2 * r;
-            __syncthreads();
-        }
-        const bool in_inside = p0 + ifirst >= 0 && p0 + NP <= n;
-        // ---- stage the chunk's new input positions -------------------------
-        if (kind == PASS_X) {
-            // lane = position along the row: 128-byte coalesced reads
-            for (int row = warp; row < 32; row += NW) {
-                const bool rowin = (rowin_mask >> row) & 1u;
-                const int sidx = 2 * (row & 15) + (row >> 4);
-                const float *src = base + (int64_t)row * sj.line_stride + p0;
-                float *dst = inf + sidx;
-                const bool fast = rowin && p0 + ifirst >= xlo && p0 + NP <= xhi;
-                constexpr int U = 4;
-                for (int i0 = ifirst + lane; i0 < NP; i0 += 32 * U) {
-                    float v[U];
-                    if (fast) {
-#pragma unroll
-                        for (int u = 0; u < U; ++u) {
-                            const int i = i0 + 32 * u;
-                            v[u] = i < NP ? __ldg(src + i) - b : 0.0f;
-                        }
-                    } else {
-#pragma unroll
-                        for (int u = 0; u < U; ++u) {
-                            const int i = i0 + 32 * u, p = p0 + i;
-                            v[u] = (rowin && i < NP && p >= xlo && p < xhi) ? __ldg(src + i) - b : 0.0f;
-                        }
-                    }
-#pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        const int i = i0 + 32 * u;
-                        if (i < NP) {
-                            dst[i * 2 * OS_LS] = v[u];
-                            acc_in += (double)v[u];  // every position is staged once
-                        }
-                    }
-                }
-            }
-        } else {
-            // lane = column: 128-byte coalesced reads of one position
-            const int sidx = 2 * (lane & 15) + (lane >> 4);
-            const bool ok = lane < nreal;
-            const float *src = base + (int64_t)lane * sj.line_stride + (int64_t)(p0 + ifirst + warp) * ps;
-            const int64_t step = (int64_t)NW * ps;
-            float *dst = inf + (ifirst + warp) * 2 * OS_LS + sidx;
-            constexpr int DST = NW * 2 * OS_LS;
-            constexpr int U = 8;
-            for (int i0 = ifirst + warp; i0 < NP; i0 += NW * U) {
-                float v[U];
-                if (in_inside) {
-#pragma unroll
-                    for (int u = 0; u < U; ++u)
-                        v[u] = (ok && i0 + NW * u < NP) ? __ldg(src + u * step) : 0.0f;
-                } else {
-#pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        const int p = p0 + i0 + NW * u;
-                        v[u] = (ok && i0 + NW * u < NP && p >= 0 && p < n) ? __ldg(src + u * step) : 0.0f;
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                    if (i0 + NW * u < NP) dst[u * DST] = v[u];
-                src += U * step;
-                dst += U * DST;
-            }
-        }
-        __syncthreads();
-
-        // ---- blocks: FFT-64, multiply, inverse, keep L samples -------------
-        const bool out_inside = c0 >= 0 && c0 + C <= n;
-        for (int u = g; u < OS_PAIRS * M; u += OS_NT / 8) {
-            // groups 2j, 2j+1 of a warp take pairs p, p + 8 (conflict-free staging reads)
-            const int pair = ((u & 1) << 3) | ((u >> 1) & 7);
-            const int seg0 = (u >> 4) * L;
-            const float2 *sp = in + (seg0 + t) * OS_LS + pair;
-            float2 x[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) x[q] = sp[q * 8 * OS_LS];
-            fft64_fwd(x, t, gs, w);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const float h = sj.H[t + 8 * k];
-                x[k] = make_float2(x[k].x * h, x[k].y * h);
-            }
-            fft64_inv(x, t, gs, w);
-            float2 *op = out + (seg0 + t - r) * OS_LS + pair;  // sample t + 8q -> out row seg0 + t + 8q - r
-            if (out_inside) {
-#pragma unroll
-                for (int q = 0; q < 8; ++q)
-                    if ((qmask >> q) & 1u) op[q * 8 * OS_LS] = x[q];
-            } else {
-                const int o0 = c0 + seg0 + t - r;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    if ((qmask >> q) & 1u) {
-                        const int o = o0 + 8 * q;
-                        if (o >= 0 && o < n) op[q * 8 * OS_LS] = x[q];
-                        else acc_leak += (double)x[q].x + (double)x[q].y;
-                    }
-                }
-            }
-        }
-        __syncthreads();
-
-        // ---- store the chunk's outputs (baseline + decay + mass in the z pass)
-        const int jlo = max(0, -c0), jhi = min(C, n - c0);
-        if (kind == PASS_X) {
-            for (int row = warp; row < nreal; row += NW) {
-                float *dst = base + (int64_t)row * sj.line_stride + c0;
-                const float *sv = outf + 2 * (row & 15) + (row >> 4);
-                for (int j = jlo + lane; j < jhi; j += 32) dst[j] = sv[j * 2 * OS_LS];
-            }
-        } else if (lane < nreal) {
-            const float *sv = outf + (jlo + warp) * 2 * OS_LS + 2 * (lane & 15) + (lane >> 4);
-            float *dst = base + (int64_t)lane * sj.line_stride + (int64_t)(c0 + jlo + warp) * ps;
-            const int64_t step = (int64_t)NW * ps;
-            if (kind == PASS_Z) {
-                const float keep = sj.keep;
-                for (int j = jlo + warp; j < jhi; j += NW) {
-                    float v = *sv;
-                    acc_conv += (double)v;
-                    v = keep * (v + b);
-                    acc_out += (double)v;
-                    *dst = v;
-                    sv += NW * 2 * OS_LS;
-                    dst += step;
-                }
-            } else {
-                for (int j = jlo + warp; j < jhi; j += NW) {
-                    *dst = *sv;
-                    sv += NW * 2 * OS_LS;
-                    dst += step;
-                }
-            }
-        }
-        // the next chunk's halo copy reads `in` (no longer read by the FFT
-        // phase) and its FFT phase writes `out` only after the next barrier
-    }
-
-    double *mass = sj.mass;
-    if (kind == PASS_X) {
-        os_block_sum(acc_in, mass + MS_INPUT, red);
-        os_block_sum(acc_leak, mass + MS_LEAK_X, red);
-    } else if (kind == PASS_Y) {
-        os_block_sum(acc_leak, mass + MS_LEAK_Y, red);
-    } else {
-        os_block_sum(acc_leak, mass + MS_LEAK_Z, red);
-        os_block_sum(acc_conv, mass + MS_CONV, red);
-        os_block_sum(acc_out, mass + MS_OUT, red);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Pipelined variant: the next chunk's new input positions are fetched with
-// cp.async (4-byte, zero-filled outside the line) into the second of two
-// staging buffers while the current chunk's FFTs run.  Used when staging
-// needs no transform on load (zero padding: v = u); the input mass of the x
-// pass is summed from the samples that are block outputs (each staged
-// position inside the chunk's output range exactly once).
-// ---------------------------------------------------------------------------
+// ---- asynchronous copies (zero-filled past the source size) ---------------
 __device__ __forceinline__ void cp_async4(float *smem, const float *gmem, bool valid)
 {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     const int n = valid ? 4 : 0;
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-// Issues the asynchronous staging of positions [ifirst, NP) of chunk (p0) into
-// stage (float view).  Rows/columns beyond nreal and positions outside
-// [0, n) are zero-filled.
-__device__ __forceinline__ void os_stage_async(float *stage, const OsJob &j, float *base, int nreal, int p0,
-                                               int ifirst, int NP)
+__device__ __forceinline__ void cp_async16(float *smem, const float *gmem, int bytes)
 {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr int NW = OS_NT / 32;
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Shared-memory geometry of one job (floats).
+struct OsGeom {
+    int NP;     // input positions of a full chunk: C + 2r
+    int delta;  // x pass: the staged window starts delta positions before the chunk's first input
+    int NPA;    // x pass: staged positions per line row (delta + NP, rounded up to 4)
+    int RS;     // x pass: floats per staged line row
+    int CS;     // x pass: floats per output line row
+    int stage;  // floats per staging buffer
+    int out;    // floats of the output staging
+};
+
+__host__ __device__ inline int os_round4mod16(int v) { return v + ((4 - v) % 16 + 16) % 16; }
+
+__host__ __device__ inline OsGeom os_geom(int r, int C, bool xpass)
+{
+    OsGeom g;
+    g.NP = C + 2 * r;
+    g.delta = xpass ? ((-r) & 3) : 0;  // x: chunk inputs start at ofirst - r + ch C = -(r + delta) mod 4
+    g.NPA = (g.delta + g.NP + 3) & ~3;
+    g.RS = os_round4mod16(g.NPA);
+    g.CS = os_round4mod16(C);
+    g.stage = xpass ? 32 * g.RS : g.NP * OS_RS;
+    g.out = xpass ? 32 * g.CS : C * OS_RS;
+    return g;
+}
+
+// Issues the asynchronous copies of staging slots [0, send) for a chunk
+// whose slot 0 is position pa.  Lines >= nreal and positions outside [0, n)
+// are zero-filled.  x pass with vec: rows 16-byte aligned, pa and n
+// multiples of 4 (a 4-position quad then lies wholly inside or outside the
+// line).  y/z with vec: positions 16-byte aligned.
+template <bool XP>
+__device__ __forceinline__ void os_stage(float *stage, const OsJob &j, const OsGeom &G, const float *base,
+                                         int nreal, int pa, int send, bool vec)
+{
     const int n = j.n;
-    if (j.kind == PASS_X) {
-        for (int row = warp; row < 32; row += NW) {
-            const bool ok = row < nreal;
-            const float *src = base + (int64_t)(ok ? row : 0) * j.line_stride;
-            float *dst = stage + 2 * (row & 15) + (row >> 4);
-            for (int i = ifirst + lane; i < NP; i += 32) {
-                const int p = p0 + i;
-                const bool v = ok && p >= 0 && p < n;
-                cp_async4(dst + i * 2 * OS_LS, v ? src + p : src, v);
+    const int64_t ls = j.line_stride, ps = j.pos_stride;
+    if (XP) {
+        if (vec) {
+            const int row = threadIdx.x >> 3, k = threadIdx.x & 7;
+            const bool rok = row < nreal;
+            const float *src = base + (rok ? row : 0) * ls;
+            float *dst = stage + row * G.RS;
+#pragma unroll 2
+            for (int s = 4 * k; s < send; s += 32) {
+                const int p = pa + s;
+                const bool v = rok && p >= 0 && p < n;
+                cp_async16(dst + s, v ? src + p : base, v ? 16 : 0);
+            }
+        } else {
+            const int wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            for (int row = wp; row < 32; row += OS_NT / 32) {
+                const bool rok = row < nreal;
+                const float *src = base + (rok ? row : 0) * ls;
+                float *dst = stage + row * G.RS;
+                for (int s = lane; s < send; s += 32) {
+                    const int p = pa + s;
+                    const bool v = rok && p >= 0 && p < n;
+                    cp_async4(dst + s, v ? src + p : base, v);
+                }
             }
         }
     } else {
-        const int64_t ps = j.pos_stride;
-        const bool ok = lane < nreal;
-        const float *src = base + (int64_t)(ok ? lane : 0) * j.line_stride;
-        float *dst = stage + 2 * (lane & 15) + (lane >> 4);
-        for (int i = ifirst + warp; i < NP; i += NW) {
-            const int p = p0 + i;
-            const bool v = ok && p >= 0 && p < n;
-            cp_async4(dst + i * 2 * OS_LS, v ? src + (int64_t)p * ps : src, v);
+        if (vec) {
+            const int k = threadIdx.x & 7, sub = threadIdx.x >> 3;
+            const int vb = 4 * min(max(nreal - 4 * k, 0), 4);
+            const float *src = base + 4 * k;
+            float *dst = stage + 4 * k;
+#pragma unroll 2
+            for (int i = sub; i < send; i += OS_NT / 8) {
+                const int p = pa + i;
+                const bool v = vb > 0 && p >= 0 && p < n;
+                cp_async16(dst + i * OS_RS, v ? src + (int64_t)p * ps : base, v ? vb : 0);
+            }
+        } else {
+            const int col = threadIdx.x & 31, wp = threadIdx.x >> 5;
+            const bool cok = col < nreal;
+            const float *src = base + (cok ? col : 0) * ls;
+            for (int i = wp; i < send; i += OS_NT / 32) {
+                const int p = pa + i;
+                const bool v = cok && p >= 0 && p < n;
+                cp_async4(stage + i * OS_RS + col, v ? src + (int64_t)p * ps : base, v);
+            }
         }
     }
 }
 
-template <int M, int MINB>
-__global__ void __launch_bounds__(OS_NT, MINB) os_pass_pipe_kernel(const OsJob *__restrict__ jobs, int njobs)
+template <bool XP>
+__global__ void __launch_bounds__(OS_NT, OS_MINB) os_pass_kernel(const OsJob *__restrict__ jobs, int njobs)
 {
-    extern __shared__ __align__(16) float2 osm[];
+    extern __shared__ __align__(16) float osm[];
     __shared__ double red[OS_NT / 32];
-    __shared__ OsJob sj;
-    __shared__ float2 tw64[64];
+    __shared__ __align__(16) OsJob sj;
+    __shared__ int sjob;
 
+    // ---- job descriptor: found by one lane, copied by its warp -------------
     const int tile = blockIdx.x;
-    if (threadIdx.x == 0) {
-        int lo = 0, hi = njobs - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (jobs[mid].tile_begin <= tile) lo = mid;
-            else hi = mid - 1;
+    if (threadIdx.x < 32) {
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = njobs - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (jobs[mid].tile_begin <= tile) lo = mid;
+                else hi = mid - 1;
+            }
+            sjob = lo;
         }
-        sj = jobs[lo];
-    }
-    if (threadIdx.x < 64) {
-        double sn, cs;
-        sincospi((double)threadIdx.x / 32.0, &sn, &cs);
-        tw64[threadIdx.x] = make_float2((float)cs, (float)-sn);
+        __syncwarp();
+        const int *src = reinterpret_cast<const int *>(jobs + sjob);
+        int *dst = reinterpret_cast<int *>(&sj);
+        for (int i = threadIdx.x; i < (int)(sizeof(OsJob) / sizeof(int)); i += 32) dst[i] = src[i];
     }
     __syncthreads();
 
     const int n = sj.n, r = sj.r, L = sj.L, C = sj.C;
-    const int NP = C + 2 * r;
-    // two staging buffers [NP][OS_LS] at osm and osm + NP * OS_LS
-    float2 *out = osm + 2 * NP * OS_LS;        // [C][OS_LS]
-    float2 *scr = out + C * OS_LS;             // [32 groups][OS_SCR]
-    float *outf = reinterpret_cast<float *>(out);
+    const OsGeom G = os_geom(r, C, XP);
+    float *const outs = osm + 2 * G.stage;
+    float2 *const scr = reinterpret_cast<float2 *>(outs + G.out);
 
     const int local = tile - sj.tile_begin;
     const int outer = local / sj.tiles_per_outer;
-    const int lt = local - outer * sj.tiles_per_outer;
-    const int l0 = lt * 32;
+    const int l0 = (local - outer * sj.tiles_per_outer) * 32;
     const int nreal = min(32, sj.nlines - l0);
-    float *base = sj.data + outer * sj.outer_stride + (int64_t)l0 * sj.line_stride;
-    const int kind = sj.kind;
+    float *const base = sj.data + outer * sj.outer_stride + (int64_t)l0 * sj.line_stride;
     const float b = sj.b;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr int NW = OS_NT / 32;
+    const int64_t ls = sj.line_stride, ps = sj.pos_stride;
+    const int nch = sj.nchunks, nblocks = sj.nblocks, ofirst = sj.ofirst;
+    const bool aligned = (reinterpret_cast<uintptr_t>(base) & 15) == 0;
+    const bool vec = XP ? (aligned && (ls & 3) == 0 && (n & 3) == 0 && (ofirst & 3) == 0)
+                        : (aligned && ls == 1 && (ps & 3) == 0);
 
+    // ---- per-lane constants of the FFT phase: group g = (pair, block) ------
+    // The 4 groups of a warp share the block, so block-uniform branches are
+    // warp-uniform (fft64_* synchronise the whole warp).
     const int g = threadIdx.x >> 3, t = threadIdx.x & 7;
-    float2 *gs = scr + g * OS_SCR;
+    const int pair = g & 15, blk = g >> 4, seg0 = blk * L;
+    float2 *const gs = scr + g * OS_SCR;
     float2 w[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) w[k] = tw64[(t * k) & 63];
-    unsigned qmask = 0;
+    for (int k = 0; k < 8; ++k) w[k] = c_tw64[(t * k) & 63];
+    unsigned qmask = 0;  // samples t + 8q that are outputs of the block
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         const int i = t + 8 * q;
         if (i >= r && i < r + L) qmask |= 1u << q;
     }
-    const int64_t ps = sj.pos_stride;
-    const int nch = sj.nchunks;
+    // constant-VF padding rule (x pass): rows of this pair inside the y/z box
+    const bool masked = XP && sj.mask;
+    bool in_a = false, in_b = false;
+    if (masked) {
+        const int la = 2 * pair;
+        if (la < nreal) {
+            const int rr = l0 + la, y = rr % sj.ny, z = rr / sj.ny;
+            in_a = y >= sj.box_lo[1] && y < sj.box_hi[1] && z >= sj.box_lo[2] && z < sj.box_hi[2];
+        }
+        if (la + 1 < nreal) {
+            const int rr = l0 + la + 1, y = rr % sj.ny, z = rr / sj.ny;
+            in_b = y >= sj.box_lo[1] && y < sj.box_hi[1] && z >= sj.box_lo[2] && z < sj.box_hi[2];
+        }
+    }
 
-    os_stage_async(reinterpret_cast<float *>(osm), sj, base, nreal, -2 * r, 0, NP);
+    // staging slots a chunk of nb blocks needs
+    auto slots = [&](int nb) { return XP ? ((G.delta + nb * L + 2 * r + 3) & ~3) : nb * L + 2 * r; };
+
+    os_stage<XP>(osm, sj, G, base, nreal, ofirst - r - G.delta, slots(min(OS_M, nblocks)), vec);
     cp_async_commit();
 
     double acc_in = 0.0, acc_leak = 0.0, acc_conv = 0.0, acc_out = 0.0;
     for (int ch = 0; ch < nch; ++ch) {
-        const int c0 = -r + ch * C, p0 = c0 - r;
-        float2 *in = osm + (ch & 1) * NP * OS_LS;
-        float2 *nxt = osm + ((ch & 1) ^ 1) * NP * OS_LS;
-        // this chunk's samples have landed; every thread has also finished the
-        // previous iteration (its halo copy out of `nxt` and its reads of `out`)
-        cp_async_wait<0>();
+        const int c0 = ofirst + ch * C, p0 = c0 - r;
+        const int nb = min(OS_M, nblocks - ch * OS_M);
+        float *const in = osm + (ch & 1) * G.stage;
+        float *const nxt = osm + ((ch & 1) ^ 1) * G.stage;
+        // chunk ch has landed, and every thread is done with the previous
+        // chunk's outputs in `outs`
+        cp_async_wait_all();
         __syncthreads();
         if (ch + 1 < nch) {
-            // next chunk: positions [2r, NP) from global memory (not yet
-            // overwritten: this chunk stores only outputs below p0 + C + 2r)
-            os_stage_async(reinterpret_cast<float *>(nxt), sj, base, nreal, p0 + C, 2 * r, NP);
+            const int pn = p0 + C;
+            os_stage<XP>(nxt, sj, G, base, nreal, pn - G.delta, slots(min(OS_M, nblocks - (ch + 1) * OS_M)), vec);
             cp_async_commit();
         }
 
-        const bool out_inside = c0 >= 0 && c0 + C <= n;
-        for (int u = g; u < OS_PAIRS * M; u += OS_NT / 8) {
-            const int pair = ((u & 1) << 3) | ((u >> 1) & 7);
-            const int seg0 = (u >> 4) * L;
-            const float2 *sp = in + (seg0 + t) * OS_LS + pair;
+        // ---- one block of one pair per group: FFT-64, multiply, inverse ----
+        if (blk < nb) {
             float2 x[8];
+            if (XP) {
+                const float *ra = in + (2 * pair) * G.RS + G.delta + seg0 + t;
+                const float *rb = ra + G.RS;
 #pragma unroll
-            for (int q = 0; q < 8; ++q) x[q] = sp[q * 8 * OS_LS];
-            if (kind == PASS_X) {
-                // input mass: the samples this block outputs (own positions)
+                for (int q = 0; q < 8; ++q) x[q] = make_float2(ra[8 * q], rb[8 * q]);
+            } else {
+                const float2 *sp = reinterpret_cast<const float2 *>(in + (seg0 + t) * OS_RS) + pair;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) x[q] = sp[q * 8 * (OS_RS / 2)];
+            }
+            if (masked) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int p = p0 + seg0 + t + 8 * q;
+                    const bool px = p >= sj.box_lo[0] && p < sj.box_hi[0];
+                    x[q].x = (in_a && px) ? x[q].x - b : 0.0f;
+                    x[q].y = (in_b && px) ? x[q].y - b : 0.0f;
+                }
+            }
+            if (XP) {
+                // input mass: each position of a line is one block's output once
+                float s = 0.0f;
 #pragma unroll
                 for (int q = 0; q < 8; ++q)
-                    if ((qmask >> q) & 1u) acc_in += (double)x[q].x + (double)x[q].y;
+                    if ((qmask >> q) & 1u) s += x[q].x + x[q].y;
+                acc_in += (double)s;
             }
             fft64_fwd(x, t, gs, w);
 #pragma unroll
@@ -480,65 +354,117 @@ __global__ void __launch_bounds__(OS_NT, MINB) os_pass_pipe_kernel(const OsJob *
                 x[k] = make_float2(x[k].x * h, x[k].y * h);
             }
             fft64_inv(x, t, gs, w);
-            float2 *op = out + (seg0 + t - r) * OS_LS + pair;
-            if (out_inside) {
+            const bool out_inside = c0 + seg0 >= 0 && c0 + seg0 + L <= n;
+            const int j0 = seg0 + t - r;  // chunk output index of sample t (q = 0)
+            float leak = 0.0f;
 #pragma unroll
-                for (int q = 0; q < 8; ++q)
-                    if ((qmask >> q) & 1u) op[q * 8 * OS_LS] = x[q];
-            } else {
-                const int o0 = c0 + seg0 + t - r;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    if ((qmask >> q) & 1u) {
-                        const int o = o0 + 8 * q;
-                        if (o >= 0 && o < n) op[q * 8 * OS_LS] = x[q];
-                        else acc_leak += (double)x[q].x + (double)x[q].y;
+            for (int q = 0; q < 8; ++q) {
+                if (!((qmask >> q) & 1u)) continue;
+                const int j = j0 + 8 * q;
+                if (!out_inside) {
+                    const int o = c0 + j;
+                    if (o < 0 || o >= n) {
+                        if (o >= -r && o < n + r) leak += x[q].x + x[q].y;
+                        continue;
                     }
                 }
+                if (XP) {
+                    outs[(2 * pair) * G.CS + j] = x[q].x;
+                    outs[(2 * pair + 1) * G.CS + j] = x[q].y;
+                } else {
+                    reinterpret_cast<float2 *>(outs + j * OS_RS)[pair] = x[q];
+                }
             }
+            acc_leak += (double)leak;
         }
+        // chunk ch+1's reads of global memory are complete (every thread)
+        // before any output of chunk ch overwrites its inputs
+        cp_async_wait_all();
         __syncthreads();
-        // carry the next chunk's first 2r positions (disjoint from its async part)
-        if (ch + 1 < nch)
-            for (int i = threadIdx.x; i < 2 * r * OS_LS; i += OS_NT) nxt[i] = in[C * OS_LS + i];
 
-        const int jlo = max(0, -c0), jhi = min(C, n - c0);
-        if (kind == PASS_X) {
-            for (int row = warp; row < nreal; row += NW) {
-                float *dst = base + (int64_t)row * sj.line_stride + c0;
-                const float *sv = outf + 2 * (row & 15) + (row >> 4);
-                for (int j = jlo + lane; j < jhi; j += 32) dst[j] = sv[j * 2 * OS_LS];
-            }
-        } else if (lane < nreal) {
-            const float *sv = outf + (jlo + warp) * 2 * OS_LS + 2 * (lane & 15) + (lane >> 4);
-            float *dst = base + (int64_t)lane * sj.line_stride + (int64_t)(c0 + jlo + warp) * ps;
-            const int64_t step = (int64_t)NW * ps;
-            if (kind == PASS_Z) {
-                const float keep = sj.keep;
-                for (int j = jlo + warp; j < jhi; j += NW) {
-                    float v = *sv;
-                    acc_conv += (double)v;
-                    v = keep * (v + b);
-                    acc_out += (double)v;
-                    *dst = v;
-                    sv += NW * 2 * OS_LS;
-                    dst += step;
+        // ---- store outputs [max(c0, 0), min(c0 + nb L, n)) ------------------
+        const int olo = max(c0, 0), ohi = min(c0 + nb * L, n);
+        if (XP) {
+            const int wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            if (vec) {
+                // olo is a multiple of 4, and so is ohi (n, or c0 + C)
+                for (int row = wp; row < nreal; row += OS_NT / 32) {
+                    float *dst = base + row * ls;
+                    const float *sv = outs + row * G.CS;  // sv[o - c0]: output at position o
+                    for (int o = olo + 4 * lane; o < ohi; o += 128) {
+                        if (o + 4 <= ohi) {
+                            *reinterpret_cast<float4 *>(dst + o) = *reinterpret_cast<const float4 *>(sv + (o - c0));
+                        } else {
+                            for (int k = o; k < ohi; ++k) dst[k] = sv[k - c0];
+                        }
+                    }
                 }
             } else {
-                for (int j = jlo + warp; j < jhi; j += NW) {
-                    *dst = *sv;
-                    sv += NW * 2 * OS_LS;
-                    dst += step;
+                for (int row = wp; row < nreal; row += OS_NT / 32) {
+                    float *dst = base + row * ls;
+                    const float *sv = outs + row * G.CS;
+                    for (int o = olo + lane; o < ohi; o += 32) dst[o] = sv[o - c0];
+                }
+            }
+        } else {
+            const int jlo = olo - c0, jhi = ohi - c0;
+            const bool last = sj.kind == PASS_Z;
+            const float keep = sj.keep;
+            if (vec) {
+                const int k = threadIdx.x & 7, sub = threadIdx.x >> 3;
+                const int valid = min(max(nreal - 4 * k, 0), 4);
+                if (valid > 0) {
+                    float *dq = base + 4 * k;
+                    for (int j = jlo + sub; j < jhi; j += OS_NT / 8) {
+                        float4 v = *reinterpret_cast<const float4 *>(outs + j * OS_RS + 4 * k);
+                        float *dst = dq + (int64_t)(c0 + j) * ps;
+                        if (last) {
+                            float sc = v.x;
+                            if (valid > 1) sc += v.y;
+                            if (valid > 2) sc += v.z;
+                            if (valid > 3) sc += v.w;
+                            acc_conv += (double)sc;
+                            v.x = keep * (v.x + b);
+                            v.y = keep * (v.y + b);
+                            v.z = keep * (v.z + b);
+                            v.w = keep * (v.w + b);
+                            float so = v.x;
+                            if (valid > 1) so += v.y;
+                            if (valid > 2) so += v.z;
+                            if (valid > 3) so += v.w;
+                            acc_out += (double)so;
+                        }
+                        if (valid == 4) {
+                            *reinterpret_cast<float4 *>(dst) = v;
+                        } else {
+                            dst[0] = v.x;
+                            if (valid > 1) dst[1] = v.y;
+                            if (valid > 2) dst[2] = v.z;
+                        }
+                    }
+                }
+            } else {
+                const int col = threadIdx.x & 31, wp = threadIdx.x >> 5;
+                if (col < nreal) {
+                    for (int j = jlo + wp; j < jhi; j += OS_NT / 32) {
+                        float v = outs[j * OS_RS + col];
+                        if (last) {
+                            acc_conv += (double)v;
+                            v = keep * (v + b);
+                            acc_out += (double)v;
+                        }
+                        base[col + (int64_t)(c0 + j) * ps] = v;
+                    }
                 }
             }
         }
     }
 
     double *mass = sj.mass;
-    if (kind == PASS_X) {
+    if (XP) {
         os_block_sum(acc_in, mass + MS_INPUT, red);
         os_block_sum(acc_leak, mass + MS_LEAK_X, red);
-    } else if (kind == PASS_Y) {
+    } else if (sj.kind == PASS_Y) {
         os_block_sum(acc_leak, mass + MS_LEAK_Y, red);
     } else {
         os_block_sum(acc_leak, mass + MS_LEAK_Z, red);
@@ -547,97 +473,70 @@ __global__ void __launch_bounds__(OS_NT, MINB) os_pass_pipe_kernel(const OsJob *
     }
 }
 
-int os_blocks_per_chunk()
+static std::mutex g_tw_mu;
+static bool g_tw_done[64];
+
+cudaError_t os_prepare()
 {
-    static int m = -1;
-    if (m < 0) {
-        const char *e = getenv("VFD_OS_M");
-        m = (e && e[0] == '4') ? 4 : 2;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_tw_mu);
+    if (g_tw_done[dev]) return cudaSuccess;
+    float2 tw[64];
+    for (int m = 0; m < 64; ++m) {
+        const double a = 6.283185307179586476925286766559 * m / 64.0;
+        tw[m] = make_float2((float)std::cos(a), (float)-std::sin(a));
     }
-    return m;
+    e = cudaMemcpyToSymbol(c_tw64, tw, sizeof(tw));
+    if (e == cudaSuccess) g_tw_done[dev] = true;
+    return e;
 }
 
-size_t os_smem_bytes(int rmin, int M)
+size_t os_smem_bytes(int rmin, int axis)
 {
-    const int L = OS_N - 2 * rmin, C = M * L;
-    return ((size_t)(C + 2 * rmin) * OS_LS + (size_t)C * OS_LS + (size_t)(OS_NT / 8) * OS_SCR) * sizeof(float2);
+    size_t best = 0;
+    for (int r = std::max(rmin, 0); r <= OS_RMAX; ++r) {
+        const OsGeom g = os_geom(r, OS_M * (OS_N - 2 * r), axis == PASS_X);
+        const size_t bytes =
+            (size_t)(2 * g.stage + g.out) * sizeof(float) + (size_t)(OS_NT / 8) * OS_SCR * sizeof(float2);
+        best = std::max(best, bytes);
+    }
+    return best;
 }
 
-template <int M, int MINB>
+template <bool XP>
 static cudaError_t launch_os_t(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st)
 {
     static thread_local int configured_dev = -1;
     int dev = 0;
     cudaGetDevice(&dev);
     if (configured_dev != dev) {
-        cudaError_t e = cudaFuncSetAttribute(os_pass_kernel<M, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(os_pass_kernel<XP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)axis_smem_limit());
         if (e != cudaSuccess) return e;
         configured_dev = dev;
     }
-    os_pass_kernel<M, MINB><<<tiles, OS_NT, os_smem_bytes(rmin, M), st>>>(jobs, njobs);
+    os_pass_kernel<XP><<<tiles, OS_NT, os_smem_bytes(rmin, XP ? PASS_X : PASS_Y), st>>>(jobs, njobs);
     note_launch();
     return cudaGetLastError();
 }
 
-static int os_min_blocks()
+cudaError_t launch_os(const OsJob *jobs, int njobs, int tiles, int rmin, int axis, cudaStream_t st)
 {
-    static int m = -1;
-    if (m < 0) {
-        const char *e = getenv("VFD_OS_MINB");
-        m = (e && e[0] == '3') ? 3 : 4;  // 4 blocks per SM (64 registers) measured faster on B200
-    }
-    return m;
-}
-
-size_t os_pipe_smem_bytes(int rmin, int M)
-{
-    const int L = OS_N - 2 * rmin, C = M * L;
-    return ((size_t)2 * (C + 2 * rmin) * OS_LS + (size_t)C * OS_LS + (size_t)(OS_NT / 8) * OS_SCR) *
-           sizeof(float2);
-}
-
-template <int M, int MINB>
-static cudaError_t launch_os_pipe_t(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st)
-{
-    static thread_local int configured_dev = -1;
+    if (tiles <= 0) return cudaSuccess;
     int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_dev != dev) {
-        cudaError_t e = cudaFuncSetAttribute(os_pass_pipe_kernel<M, MINB>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axis_smem_limit());
-        if (e != cudaSuccess) return e;
-        configured_dev = dev;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    bool ready;
+    {
+        std::lock_guard<std::mutex> lk(g_tw_mu);
+        ready = dev >= 0 && dev < 64 && g_tw_done[dev];
     }
-    os_pass_pipe_kernel<M, MINB><<<tiles, OS_NT, os_pipe_smem_bytes(rmin, M), st>>>(jobs, njobs);
-    note_launch();
-    return cudaGetLastError();
-}
-
-bool os_pipe_enabled()
-{
-    static int on = -1;
-    if (on < 0) {
-        const char *e = getenv("VFD_OS_PIPE");
-        on = (e && e[0] == '0') ? 0 : 1;
-    }
-    return on == 1;
-}
-
-cudaError_t launch_os_pipe(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st)
-{
-    if (tiles <= 0) return cudaSuccess;
-    // the pipelined kernel measured fastest at 3 blocks per SM (80 registers)
-    if (os_blocks_per_chunk() == 4) return launch_os_pipe_t<4, 2>(jobs, njobs, tiles, rmin, st);
-    return launch_os_pipe_t<2, 3>(jobs, njobs, tiles, rmin, st);
-}
-
-cudaError_t launch_os(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st)
-{
-    if (tiles <= 0) return cudaSuccess;
-    if (os_blocks_per_chunk() == 4) return launch_os_t<4, 2>(jobs, njobs, tiles, rmin, st);
-    if (os_min_blocks() == 4) return launch_os_t<2, 4>(jobs, njobs, tiles, rmin, st);
-    return launch_os_t<2, 3>(jobs, njobs, tiles, rmin, st);
+    if (!ready && (e = os_prepare()) != cudaSuccess) return e;
+    if (axis == PASS_X) return launch_os_t<true>(jobs, njobs, tiles, rmin, st);
+    return launch_os_t<false>(jobs, njobs, tiles, rmin, st);
 }
 
 }  // namespace vfd

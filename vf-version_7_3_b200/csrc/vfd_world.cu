@@ -200,7 +200,6 @@ struct vfd_world {
     int tiles_per_field[3] = {0, 0, 0};
     // overlap-save passes (kernel radius <= OS_RMAX): per axis
     bool use_os[3] = {false, false, false};
-    bool os_pipe[3] = {false, false, false};  // staging needs no transform: pipelined kernel
     int rmin[3] = {0, 0, 0};
     OsJob *d_osjobs = nullptr;             // [pass][nf] all-field, then [pass][nf] single-field
     std::vector<int> os_tiles[3];          // per field
@@ -371,6 +370,8 @@ static bool os_enabled()
     return on == 1;
 }
 
+static bool os_plain_staging(const OsJob &j);
+
 static OsJob make_os_job(const vfd_world *w, int f, int a, int tile_begin)
 {
     const AxisJob aj = make_job(w, f, a, 0, 16);
@@ -386,8 +387,10 @@ static OsJob make_os_job(const vfd_world *w, int f, int a, int tile_begin)
     j.nouter = aj.nouter;
     j.r = w->params[f].radius[a];
     j.L = OS_N - 2 * j.r;
-    j.C = os_blocks_per_chunk() * j.L;
-    j.nchunks = (j.n + 2 * j.r + j.C - 1) / j.C;
+    j.C = OS_M * j.L;
+    j.ofirst = os_first_output(j.r, a);
+    j.nblocks = (j.n + j.r - j.ofirst + j.L - 1) / j.L;
+    j.nchunks = (j.nblocks + OS_M - 1) / OS_M;
     j.tiles_per_outer = (j.nlines + 31) / 32;
     j.tile_begin = tile_begin;
     j.kind = a;
@@ -399,6 +402,7 @@ static OsJob make_os_job(const vfd_world *w, int f, int a, int tile_begin)
         j.box_lo[i] = aj.box_lo[i];
         j.box_hi[i] = aj.box_hi[i];
     }
+    j.mask = os_plain_staging(j) ? 0 : 1;
     std::vector<float> h;
     gauss_spectrum(w->params[f].sigma[a], j.r, OS_N, h);
     for (int k = 0; k < OS_N; ++k) j.H[k] = h[k];
@@ -596,16 +600,15 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
         for (int a = 0; a < 3; ++a) {
             int tb = 0;
             w->os_tiles[a].assign(w->nf, 0);
-            w->os_pipe[a] = os_pipe_enabled();
             for (int f = 0; f < w->nf; ++f) {
                 oj.push_back(make_os_job(w, f, a, tb));
                 w->os_tiles[a][f] = os_field_tiles(oj.back());
-                w->os_pipe[a] = w->os_pipe[a] && os_plain_staging(oj.back());
                 tb += w->os_tiles[a][f];
             }
         }
         for (int a = 0; a < 3; ++a)
             for (int f = 0; f < w->nf; ++f) oj.push_back(make_os_job(w, f, a, 0));
+        if ((e = os_prepare()) != cudaSuccess) return bail(e, "overlap-save twiddles");
         if ((e = cudaMalloc(&w->d_osjobs, sizeof(OsJob) * oj.size())) != cudaSuccess) return bail(e, "cudaMalloc os jobs");
         if ((e = cudaMemcpy(w->d_osjobs, oj.data(), sizeof(OsJob) * oj.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
             return bail(e, "cudaMemcpy os jobs");
@@ -1065,8 +1068,7 @@ static vfd_status enqueue_tick(vfd_world *w, int field, int n_substeps, cudaStre
                     for (int f = 0; f < w->nf; ++f) tiles += w->os_tiles[a][f];
                 else
                     tiles = w->os_tiles[a][field];
-                if (w->os_pipe[a]) VFD_CUDA(w, launch_os_pipe(jobs, nj, tiles, w->rmin[a], st));
-                else VFD_CUDA(w, launch_os(jobs, nj, tiles, w->rmin[a], st));
+                VFD_CUDA(w, launch_os(jobs, nj, tiles, w->rmin[a], a, st));
             } else {
                 const AxisJob *jobs = field < 0 ? w->d_jobs + a * w->nf : w->d_jobs + 3 * w->nf + a * w->nf + field;
                 const int tiles = w->tiles_per_field[a] * nj;
@@ -1232,7 +1234,6 @@ struct vfd_batch {
     int njobs = 0;
     AxisJob *d_jobs = nullptr;  // [3][njobs]
     bool use_os[3] = {false, false, false};
-    bool os_pipe[3] = {false, false, false};
     int rmin[3] = {0, 0, 0};
     OsJob *d_osjobs = nullptr;  // [3][njobs]
     int os_tiles[3] = {0, 0, 0};
@@ -1332,11 +1333,9 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
     if (b->use_os[0] || b->use_os[1] || b->use_os[2]) {
         for (int a = 0; a < 3; ++a) {
             int tb = 0;
-            b->os_pipe[a] = os_pipe_enabled();
             for (auto *w : b->worlds)
                 for (int f = 0; f < w->nf; ++f) {
                     oj.push_back(make_os_job(w, f, a, tb));
-                    b->os_pipe[a] = b->os_pipe[a] && os_plain_staging(oj.back());
                     tb += os_field_tiles(oj.back());
                 }
             b->os_tiles[a] = tb;
@@ -1344,8 +1343,9 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
     }
     DeviceGuard g(b->device);
     if (!oj.empty()) {
-        cudaError_t e2;
-        if ((e2 = cudaMalloc(&b->d_osjobs, sizeof(OsJob) * oj.size())) != cudaSuccess ||
+        cudaError_t e2 = cudaSuccess;
+        if ((e2 = os_prepare()) != cudaSuccess ||
+            (e2 = cudaMalloc(&b->d_osjobs, sizeof(OsJob) * oj.size())) != cudaSuccess ||
             (e2 = cudaMemcpy(b->d_osjobs, oj.data(), sizeof(OsJob) * oj.size(), cudaMemcpyHostToDevice)) != cudaSuccess) {
             std::string msg = std::string("batch os jobs: ") + cudaGetErrorString(e2);
             batch_release(b);
@@ -1383,11 +1383,8 @@ static vfd_status batch_enqueue(vfd_batch *b, int n_substeps)
         for (auto *w : b->worlds)
             VFD_BCUDA(b, cudaMemsetAsync(w->d_mass, 0, sizeof(double) * MS_COUNT * w->nf, b->st));
         for (int a = 0; a < 3; ++a) {
-            if (b->use_os[a] && b->os_pipe[a])
-                VFD_BCUDA(b, launch_os_pipe(b->d_osjobs + a * b->njobs, b->njobs, b->os_tiles[a], b->rmin[a],
-                                            b->st));
-            else if (b->use_os[a])
-                VFD_BCUDA(b, launch_os(b->d_osjobs + a * b->njobs, b->njobs, b->os_tiles[a], b->rmin[a], b->st));
+            if (b->use_os[a])
+                VFD_BCUDA(b, launch_os(b->d_osjobs + a * b->njobs, b->njobs, b->os_tiles[a], b->rmin[a], a, b->st));
             else
                 VFD_BCUDA(b, launch_axis(b->variant[a], b->d_jobs + a * b->njobs, b->njobs, b->tiles[a],
                                          b->Fmax[a], b->st));
