@@ -59,9 +59,8 @@
 namespace vfd {
 
 constexpr int OS_NT = 256;      // threads per CTA: 32 groups of 8 lanes
-constexpr int OS_SCR = 64 + 8;  // float2 per group scratch (64 + pad)
+constexpr int OS_SCR = 72;      // float2 per group scratch: 8 rows of 9
 constexpr int OS_RS = 36;       // y/z staging: floats per position row
-constexpr int OS_MINB = 3;      // CTAs per SM (80 registers per thread)
 
 __constant__ float2 c_tw64[64];  // exp(-2 pi i m / 64), FP64-generated on the host
 
@@ -86,37 +85,90 @@ __device__ __forceinline__ void os_block_sum(double v, double *dst, double *red)
     __syncthreads();
 }
 
-// Forward FFT-64 of the 8 samples x[q] = s[t + 8q] of lane t of a group;
-// on return lane t holds bins t + 8 k2 in x[k2].  scr: the group's scratch.
-// All 32 lanes of the warp call it together (__syncwarp).
-__device__ __forceinline__ void fft64_fwd(float2 (&x)[8], int t, float2 *scr, const float2 (&w)[8])
+// ---- packed FP32x2 complex arithmetic (one instruction per complex add,
+// subtract or real scale; a - b is fma(b, -1, a), rounded once like a - b) --
+__device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 p_sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+__device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+
+// DFT-4 in place; forward uses w4 = -i, inverse +i.
+template <bool INV>
+__device__ __forceinline__ void dft4p(float2 &a0, float2 &a1, float2 &a2, float2 &a3)
 {
-    Dft<8, false>::run(x);
+    const float2 t0 = p_add(a0, a2), t1 = p_sub(a0, a2);
+    const float2 t2 = p_add(a1, a3), d = p_sub(a1, a3);
+    a0 = p_add(t0, t2);
+    a2 = p_sub(t0, t2);
+    if (!INV) {  // t3 = -i d
+        a1 = make_float2(t1.x + d.y, t1.y - d.x);
+        a3 = make_float2(t1.x - d.y, t1.y + d.x);
+    } else {     // t3 = +i d
+        a1 = make_float2(t1.x - d.y, t1.y + d.x);
+        a3 = make_float2(t1.x + d.y, t1.y - d.x);
+    }
+}
+
+// DFT-8 in place (radix 2 x 4), w8 = exp(-+ i pi / 4).
+template <bool INV>
+__device__ __forceinline__ void dft8p(float2 (&v)[8])
+{
+    const float h = 0.707106781186547524400844362105f;
+    float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4p<INV>(e0, e1, e2, e3);
+    dft4p<INV>(o0, o1, o2, o3);
+    if (!INV) {
+        o1 = p_mul(make_float2(o1.x + o1.y, o1.y - o1.x), make_float2(h, h));
+        o3 = p_mul(make_float2(o3.y - o3.x, o3.x + o3.y), make_float2(h, -h));
+        v[2] = make_float2(e2.x + o2.y, e2.y - o2.x);  // o2 * -i
+        v[6] = make_float2(e2.x - o2.y, e2.y + o2.x);
+    } else {
+        o1 = p_mul(make_float2(o1.x - o1.y, o1.x + o1.y), make_float2(h, h));
+        o3 = p_mul(make_float2(o3.x + o3.y, o3.x - o3.y), make_float2(-h, h));
+        v[2] = make_float2(e2.x - o2.y, e2.y + o2.x);  // o2 * +i
+        v[6] = make_float2(e2.x + o2.y, e2.y - o2.x);
+    }
+    v[0] = p_add(e0, o0);
+    v[4] = p_sub(e0, o0);
+    v[1] = p_add(e1, o1);
+    v[5] = p_sub(e1, o1);
+    v[3] = p_add(e3, o3);
+    v[7] = p_sub(e3, o3);
+}
+
+// Forward FFT-64 of the 8 samples x[q] = s[t + 8q] of lane t of a group;
+// on return lane t holds bins t + 8 k2 in x[k2].  The group's scratch is 8
+// rows of 9 float2; lane t writes column t (wr = scr + t) and reads row t
+// (rd = scr + 9t), so every access is a base plus a constant offset.  All 32
+// lanes of the warp call it together (__syncwarp).
+__device__ __forceinline__ void fft64_fwd(float2 (&x)[8], float2 *wr, const float2 *rd, const float2 (&w)[8])
+{
+    dft8p<false>(x);
 #pragma unroll
     for (int k = 1; k < 8; ++k) x[k] = c_mul(x[k], w[k]);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) scr[k * 8 + ((t + k) & 7)] = x[k];
+    for (int k = 0; k < 8; ++k) wr[9 * k] = x[k];
     __syncwarp();
 #pragma unroll
-    for (int s = 0; s < 8; ++s) x[s] = scr[t * 8 + ((s + t) & 7)];
+    for (int s = 0; s < 8; ++s) x[s] = rd[s];
     __syncwarp();
-    Dft<8, false>::run(x);
+    dft8p<false>(x);
 }
 
 // Inverse of fft64_fwd (unnormalised): lane t, x[k2] = bin t + 8 k2 in,
 // samples t + 8q out in x[q].
-__device__ __forceinline__ void fft64_inv(float2 (&x)[8], int t, float2 *scr, const float2 (&w)[8])
+__device__ __forceinline__ void fft64_inv(float2 (&x)[8], float2 *wr, const float2 *rd, const float2 (&w)[8])
 {
-    Dft<8, true>::run(x);
+    dft8p<true>(x);
 #pragma unroll
-    for (int s = 0; s < 8; ++s) scr[t * 8 + ((s + t) & 7)] = x[s];
+    for (int s = 0; s < 8; ++s) wr[9 * s] = x[s];
     __syncwarp();
 #pragma unroll
-    for (int k = 0; k < 8; ++k) x[k] = scr[k * 8 + ((t + k) & 7)];
+    for (int k = 0; k < 8; ++k) x[k] = rd[k];
     __syncwarp();
 #pragma unroll
     for (int k = 1; k < 8; ++k) x[k] = c_mul(x[k], make_float2(w[k].x, -w[k].y));
-    Dft<8, true>::run(x);
+    dft8p<true>(x);
 }
 
 // ---- asynchronous copies (zero-filled past the source size) ---------------
@@ -138,11 +190,8 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 struct OsGeom {
     int NP;     // input positions of a full chunk: C + 2r
     int delta;  // x pass: the staged window starts delta positions before the chunk's first input
-    int NPA;    // x pass: staged positions per line row (delta + NP, rounded up to 4)
     int RS;     // x pass: floats per staged line row
-    int CS;     // x pass: floats per output line row
     int stage;  // floats per staging buffer
-    int out;    // floats of the output staging
 };
 
 __host__ __device__ inline int os_round4mod16(int v) { return v + ((4 - v) % 16 + 16) % 16; }
@@ -152,22 +201,19 @@ __host__ __device__ inline OsGeom os_geom(int r, int C, bool xpass)
     OsGeom g;
     g.NP = C + 2 * r;
     g.delta = xpass ? ((-r) & 3) : 0;  // x: chunk inputs start at ofirst - r + ch C = -(r + delta) mod 4
-    g.NPA = (g.delta + g.NP + 3) & ~3;
-    g.RS = os_round4mod16(g.NPA);
-    g.CS = os_round4mod16(C);
+    g.RS = os_round4mod16((g.delta + g.NP + 3) & ~3);
     g.stage = xpass ? 32 * g.RS : g.NP * OS_RS;
-    g.out = xpass ? 32 * g.CS : C * OS_RS;
     return g;
 }
 
-// Issues the asynchronous copies of staging slots [0, send) for a chunk
+// Issues the asynchronous copies of staging slots [sfirst, send) for a chunk
 // whose slot 0 is position pa.  Lines >= nreal and positions outside [0, n)
-// are zero-filled.  x pass with vec: rows 16-byte aligned, pa and n
+// are zero-filled.  x pass with vec: rows 16-byte aligned, pa, sfirst and n
 // multiples of 4 (a 4-position quad then lies wholly inside or outside the
 // line).  y/z with vec: positions 16-byte aligned.
 template <bool XP>
 __device__ __forceinline__ void os_stage(float *stage, const OsJob &j, const OsGeom &G, const float *base,
-                                         int nreal, int pa, int send, bool vec)
+                                         int nreal, int pa, int sfirst, int send, bool vec)
 {
     const int n = j.n;
     const int64_t ls = j.line_stride, ps = j.pos_stride;
@@ -178,7 +224,7 @@ __device__ __forceinline__ void os_stage(float *stage, const OsJob &j, const OsG
             const float *src = base + (rok ? row : 0) * ls;
             float *dst = stage + row * G.RS;
 #pragma unroll 2
-            for (int s = 4 * k; s < send; s += 32) {
+            for (int s = sfirst + 4 * k; s < send; s += 32) {
                 const int p = pa + s;
                 const bool v = rok && p >= 0 && p < n;
                 cp_async16(dst + s, v ? src + p : base, v ? 16 : 0);
@@ -189,7 +235,7 @@ __device__ __forceinline__ void os_stage(float *stage, const OsJob &j, const OsG
                 const bool rok = row < nreal;
                 const float *src = base + (rok ? row : 0) * ls;
                 float *dst = stage + row * G.RS;
-                for (int s = lane; s < send; s += 32) {
+                for (int s = sfirst + lane; s < send; s += 32) {
                     const int p = pa + s;
                     const bool v = rok && p >= 0 && p < n;
                     cp_async4(dst + s, v ? src + p : base, v);
@@ -203,7 +249,7 @@ __device__ __forceinline__ void os_stage(float *stage, const OsJob &j, const OsG
             const float *src = base + 4 * k;
             float *dst = stage + 4 * k;
 #pragma unroll 2
-            for (int i = sub; i < send; i += OS_NT / 8) {
+            for (int i = sfirst + sub; i < send; i += OS_NT / 8) {
                 const int p = pa + i;
                 const bool v = vb > 0 && p >= 0 && p < n;
                 cp_async16(dst + i * OS_RS, v ? src + (int64_t)p * ps : base, v ? vb : 0);
@@ -212,7 +258,7 @@ __device__ __forceinline__ void os_stage(float *stage, const OsJob &j, const OsG
             const int col = threadIdx.x & 31, wp = threadIdx.x >> 5;
             const bool cok = col < nreal;
             const float *src = base + (cok ? col : 0) * ls;
-            for (int i = wp; i < send; i += OS_NT / 32) {
+            for (int i = sfirst + wp; i < send; i += OS_NT / 32) {
                 const int p = pa + i;
                 const bool v = cok && p >= 0 && p < n;
                 cp_async4(stage + i * OS_RS + col, v ? src + (int64_t)p * ps : base, v);
@@ -221,12 +267,13 @@ __device__ __forceinline__ void os_stage(float *stage, const OsJob &j, const OsG
     }
 }
 
-template <bool XP>
-__global__ void __launch_bounds__(OS_NT, OS_MINB) os_pass_kernel(const OsJob *__restrict__ jobs, int njobs)
+template <bool XP, int MINB>
+__global__ void __launch_bounds__(OS_NT, MINB) os_pass_kernel(const OsJob *__restrict__ jobs, int njobs)
 {
     extern __shared__ __align__(16) float osm[];
     __shared__ double red[OS_NT / 32];
     __shared__ __align__(16) OsJob sj;
+    __shared__ __align__(16) float2 hh[OS_N];  // (H[k], H[k]) for packed scaling
     __shared__ int sjob;
 
     // ---- job descriptor: found by one lane, copied by its warp -------------
@@ -247,18 +294,17 @@ __global__ void __launch_bounds__(OS_NT, OS_MINB) os_pass_kernel(const OsJob *__
         for (int i = threadIdx.x; i < (int)(sizeof(OsJob) / sizeof(int)); i += 32) dst[i] = src[i];
     }
     __syncthreads();
+    if (threadIdx.x < OS_N) hh[threadIdx.x] = make_float2(sj.H[threadIdx.x], sj.H[threadIdx.x]);
 
     const int n = sj.n, r = sj.r, L = sj.L, C = sj.C;
     const OsGeom G = os_geom(r, C, XP);
-    float *const outs = osm + 2 * G.stage;
-    float2 *const scr = reinterpret_cast<float2 *>(outs + G.out);
+    const int hs = r + G.delta;  // slots a chunk carries over from the previous one (x: a multiple of 4)
 
     const int local = tile - sj.tile_begin;
     const int outer = local / sj.tiles_per_outer;
     const int l0 = (local - outer * sj.tiles_per_outer) * 32;
     const int nreal = min(32, sj.nlines - l0);
     float *const base = sj.data + outer * sj.outer_stride + (int64_t)l0 * sj.line_stride;
-    const float b = sj.b;
     const int64_t ls = sj.line_stride, ps = sj.pos_stride;
     const int nch = sj.nchunks, nblocks = sj.nblocks, ofirst = sj.ofirst;
     const bool aligned = (reinterpret_cast<uintptr_t>(base) & 15) == 0;
@@ -270,7 +316,9 @@ __global__ void __launch_bounds__(OS_NT, OS_MINB) os_pass_kernel(const OsJob *__
     // warp-uniform (fft64_* synchronise the whole warp).
     const int g = threadIdx.x >> 3, t = threadIdx.x & 7;
     const int pair = g & 15, blk = g >> 4, seg0 = blk * L;
-    float2 *const gs = scr + g * OS_SCR;
+    float2 *const gs = reinterpret_cast<float2 *>(osm + 2 * G.stage) + g * OS_SCR;
+    float2 *const wr = gs + t;
+    const float2 *const rd = gs + 9 * t;
     float2 w[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) w[k] = c_tw64[(t * k) & 63];
@@ -280,25 +328,30 @@ __global__ void __launch_bounds__(OS_NT, OS_MINB) os_pass_kernel(const OsJob *__
         const int i = t + 8 * q;
         if (i >= r && i < r + L) qmask |= 1u << q;
     }
+    const bool va = 2 * pair < nreal, vb = 2 * pair + 1 < nreal;  // real lines of this pair
+    // y/z outputs of a pair go out as one 8-byte store when aligned
+    const bool st2 = !XP && vb && ((reinterpret_cast<uintptr_t>(base) & 7) == 0) && ((ps & 1) == 0);
     // constant-VF padding rule (x pass): rows of this pair inside the y/z box
     const bool masked = XP && sj.mask;
+    const float b = sj.b;
     bool in_a = false, in_b = false;
     if (masked) {
-        const int la = 2 * pair;
-        if (la < nreal) {
-            const int rr = l0 + la, y = rr % sj.ny, z = rr / sj.ny;
+        if (va) {
+            const int rr = l0 + 2 * pair, y = rr % sj.ny, z = rr / sj.ny;
             in_a = y >= sj.box_lo[1] && y < sj.box_hi[1] && z >= sj.box_lo[2] && z < sj.box_hi[2];
         }
-        if (la + 1 < nreal) {
-            const int rr = l0 + la + 1, y = rr % sj.ny, z = rr / sj.ny;
+        if (vb) {
+            const int rr = l0 + 2 * pair + 1, y = rr % sj.ny, z = rr / sj.ny;
             in_b = y >= sj.box_lo[1] && y < sj.box_hi[1] && z >= sj.box_lo[2] && z < sj.box_hi[2];
         }
     }
+    const bool zlast = !XP && sj.kind == PASS_Z;
+    const float2 keep2 = make_float2(sj.keep, sj.keep), b2 = make_float2(b, b);
 
     // staging slots a chunk of nb blocks needs
     auto slots = [&](int nb) { return XP ? ((G.delta + nb * L + 2 * r + 3) & ~3) : nb * L + 2 * r; };
 
-    os_stage<XP>(osm, sj, G, base, nreal, ofirst - r - G.delta, slots(min(OS_M, nblocks)), vec);
+    os_stage<XP>(osm, sj, G, base, nreal, ofirst - r - G.delta, 0, slots(min(OS_M, nblocks)), vec);
     cp_async_commit();
 
     double acc_in = 0.0, acc_leak = 0.0, acc_conv = 0.0, acc_out = 0.0;
@@ -307,17 +360,33 @@ __global__ void __launch_bounds__(OS_NT, OS_MINB) os_pass_kernel(const OsJob *__
         const int nb = min(OS_M, nblocks - ch * OS_M);
         float *const in = osm + (ch & 1) * G.stage;
         float *const nxt = osm + ((ch & 1) ^ 1) * G.stage;
-        // chunk ch has landed, and every thread is done with the previous
-        // chunk's outputs in `outs`
+        // chunk ch has landed (copies and carried slots), and every thread is
+        // done with the previous chunk (its reads of `nxt`)
         cp_async_wait_all();
         __syncthreads();
         if (ch + 1 < nch) {
-            const int pn = p0 + C;
-            os_stage<XP>(nxt, sj, G, base, nreal, pn - G.delta, slots(min(OS_M, nblocks - (ch + 1) * OS_M)), vec);
+            // next chunk, slots [hs, ..): positions >= c0 + C, which this
+            // chunk does not store
+            os_stage<XP>(nxt, sj, G, base, nreal, p0 + C - G.delta, hs, slots(min(OS_M, nblocks - (ch + 1) * OS_M)),
+                         vec);
             cp_async_commit();
+            // slots [0, hs): inputs this chunk overwrites, carried in shared memory
+            if (XP) {
+                const int q4 = hs >> 2;
+                for (int i = threadIdx.x; i < 32 * q4; i += OS_NT) {
+                    const int row = i / q4, c = i - row * q4;
+                    reinterpret_cast<float4 *>(nxt + row * G.RS)[c] =
+                        reinterpret_cast<const float4 *>(in + row * G.RS + C)[c];
+                }
+            } else {
+                const float4 *hsrc = reinterpret_cast<const float4 *>(in + C * OS_RS);
+                float4 *hdst = reinterpret_cast<float4 *>(nxt);
+                for (int i = threadIdx.x; i < hs * (OS_RS / 4); i += OS_NT) hdst[i] = hsrc[i];
+            }
         }
 
-        // ---- one block of one pair per group: FFT-64, multiply, inverse ----
+        // ---- one block of one pair per group: FFT-64, multiply, inverse,
+        // outputs straight to global memory -------------------------------
         if (blk < nb) {
             float2 x[8];
             if (XP) {
@@ -341,121 +410,63 @@ __global__ void __launch_bounds__(OS_NT, OS_MINB) os_pass_kernel(const OsJob *__
             }
             if (XP) {
                 // input mass: each position of a line is one block's output once
-                float s = 0.0f;
+                float2 s2 = make_float2(0.0f, 0.0f);
 #pragma unroll
                 for (int q = 0; q < 8; ++q)
-                    if ((qmask >> q) & 1u) s += x[q].x + x[q].y;
-                acc_in += (double)s;
+                    if ((qmask >> q) & 1u) s2 = p_add(s2, x[q]);
+                acc_in += (double)((va ? s2.x : 0.0f) + (vb ? s2.y : 0.0f));
             }
-            fft64_fwd(x, t, gs, w);
+            fft64_fwd(x, wr, rd, w);
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const float h = sj.H[t + 8 * k];
-                x[k] = make_float2(x[k].x * h, x[k].y * h);
-            }
-            fft64_inv(x, t, gs, w);
-            const bool out_inside = c0 + seg0 >= 0 && c0 + seg0 + L <= n;
-            const int j0 = seg0 + t - r;  // chunk output index of sample t (q = 0)
-            float leak = 0.0f;
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                if (!((qmask >> q) & 1u)) continue;
-                const int j = j0 + 8 * q;
-                if (!out_inside) {
-                    const int o = c0 + j;
-                    if (o < 0 || o >= n) {
-                        if (o >= -r && o < n + r) leak += x[q].x + x[q].y;
-                        continue;
-                    }
-                }
-                if (XP) {
-                    outs[(2 * pair) * G.CS + j] = x[q].x;
-                    outs[(2 * pair + 1) * G.CS + j] = x[q].y;
-                } else {
-                    reinterpret_cast<float2 *>(outs + j * OS_RS)[pair] = x[q];
-                }
-            }
-            acc_leak += (double)leak;
-        }
-        // chunk ch+1's reads of global memory are complete (every thread)
-        // before any output of chunk ch overwrites its inputs
-        cp_async_wait_all();
-        __syncthreads();
+            for (int k = 0; k < 8; ++k) x[k] = p_mul(x[k], hh[t + 8 * k]);
+            fft64_inv(x, wr, rd, w);
 
-        // ---- store outputs [max(c0, 0), min(c0 + nb L, n)) ------------------
-        const int olo = max(c0, 0), ohi = min(c0 + nb * L, n);
-        if (XP) {
-            const int wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-            if (vec) {
-                // olo is a multiple of 4, and so is ohi (n, or c0 + C)
-                for (int row = wp; row < nreal; row += OS_NT / 32) {
-                    float *dst = base + row * ls;
-                    const float *sv = outs + row * G.CS;  // sv[o - c0]: output at position o
-                    for (int o = olo + 4 * lane; o < ohi; o += 128) {
-                        if (o + 4 <= ohi) {
-                            *reinterpret_cast<float4 *>(dst + o) = *reinterpret_cast<const float4 *>(sv + (o - c0));
-                        } else {
-                            for (int k = o; k < ohi; ++k) dst[k] = sv[k - c0];
-                        }
+            const int ob = c0 + seg0 + t - r;  // position of sample t (q = 0)
+            const bool inside = c0 + seg0 >= 0 && c0 + seg0 + L <= n;
+            float2 lk2 = make_float2(0.0f, 0.0f), cv2 = lk2, ot2 = lk2;
+            if (XP) {
+                float *da = base + (2 * pair) * ls;
+                float *db = da + ls;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    if (!((qmask >> q) & 1u)) continue;
+                    const int o = ob + 8 * q;
+                    if (inside || (o >= 0 && o < n)) {
+                        if (va) da[o] = x[q].x;
+                        if (vb) db[o] = x[q].y;
+                    } else if (o >= -r && o < n + r) {
+                        lk2 = p_add(lk2, x[q]);
                     }
                 }
             } else {
-                for (int row = wp; row < nreal; row += OS_NT / 32) {
-                    float *dst = base + row * ls;
-                    const float *sv = outs + row * G.CS;
-                    for (int o = olo + lane; o < ohi; o += 32) dst[o] = sv[o - c0];
+                float *d = base + 2 * pair + (int64_t)ob * ps;
+                const int64_t step = 8 * ps;
+#pragma unroll
+                for (int q = 0; q < 8; ++q, d += step) {
+                    if (!((qmask >> q) & 1u)) continue;
+                    const int o = ob + 8 * q;
+                    if (inside || (o >= 0 && o < n)) {
+                        float2 v = x[q];
+                        if (zlast) {
+                            cv2 = p_add(cv2, v);
+                            v = p_mul(p_add(v, b2), keep2);
+                            ot2 = p_add(ot2, v);
+                        }
+                        if (st2) {
+                            *reinterpret_cast<float2 *>(d) = v;
+                        } else {
+                            if (va) d[0] = v.x;
+                            if (vb) d[1] = v.y;
+                        }
+                    } else if (o >= -r && o < n + r) {
+                        lk2 = p_add(lk2, x[q]);
+                    }
                 }
             }
-        } else {
-            const int jlo = olo - c0, jhi = ohi - c0;
-            const bool last = sj.kind == PASS_Z;
-            const float keep = sj.keep;
-            if (vec) {
-                const int k = threadIdx.x & 7, sub = threadIdx.x >> 3;
-                const int valid = min(max(nreal - 4 * k, 0), 4);
-                if (valid > 0) {
-                    float *dq = base + 4 * k;
-                    for (int j = jlo + sub; j < jhi; j += OS_NT / 8) {
-                        float4 v = *reinterpret_cast<const float4 *>(outs + j * OS_RS + 4 * k);
-                        float *dst = dq + (int64_t)(c0 + j) * ps;
-                        if (last) {
-                            float sc = v.x;
-                            if (valid > 1) sc += v.y;
-                            if (valid > 2) sc += v.z;
-                            if (valid > 3) sc += v.w;
-                            acc_conv += (double)sc;
-                            v.x = keep * (v.x + b);
-                            v.y = keep * (v.y + b);
-                            v.z = keep * (v.z + b);
-                            v.w = keep * (v.w + b);
-                            float so = v.x;
-                            if (valid > 1) so += v.y;
-                            if (valid > 2) so += v.z;
-                            if (valid > 3) so += v.w;
-                            acc_out += (double)so;
-                        }
-                        if (valid == 4) {
-                            *reinterpret_cast<float4 *>(dst) = v;
-                        } else {
-                            dst[0] = v.x;
-                            if (valid > 1) dst[1] = v.y;
-                            if (valid > 2) dst[2] = v.z;
-                        }
-                    }
-                }
-            } else {
-                const int col = threadIdx.x & 31, wp = threadIdx.x >> 5;
-                if (col < nreal) {
-                    for (int j = jlo + wp; j < jhi; j += OS_NT / 32) {
-                        float v = outs[j * OS_RS + col];
-                        if (last) {
-                            acc_conv += (double)v;
-                            v = keep * (v + b);
-                            acc_out += (double)v;
-                        }
-                        base[col + (int64_t)(c0 + j) * ps] = v;
-                    }
-                }
+            acc_leak += (double)((va ? lk2.x : 0.0f) + (vb ? lk2.y : 0.0f));
+            if (zlast) {
+                acc_conv += (double)((va ? cv2.x : 0.0f) + (vb ? cv2.y : 0.0f));
+                acc_out += (double)((va ? ot2.x : 0.0f) + (vb ? ot2.y : 0.0f));
             }
         }
     }
@@ -499,26 +510,35 @@ size_t os_smem_bytes(int rmin, int axis)
     size_t best = 0;
     for (int r = std::max(rmin, 0); r <= OS_RMAX; ++r) {
         const OsGeom g = os_geom(r, OS_M * (OS_N - 2 * r), axis == PASS_X);
-        const size_t bytes =
-            (size_t)(2 * g.stage + g.out) * sizeof(float) + (size_t)(OS_NT / 8) * OS_SCR * sizeof(float2);
+        const size_t bytes = (size_t)(2 * g.stage) * sizeof(float) + (size_t)(OS_NT / 8) * OS_SCR * sizeof(float2);
         best = std::max(best, bytes);
     }
     return best;
 }
 
-template <bool XP>
+static int os_min_blocks()
+{
+    static int m = -1;
+    if (m < 0) {
+        const char *ev = getenv("VFD_OS_MINB");
+        m = (ev && ev[0] == '4') ? 4 : 3;
+    }
+    return m;
+}
+
+template <bool XP, int MINB>
 static cudaError_t launch_os_t(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st)
 {
     static thread_local int configured_dev = -1;
     int dev = 0;
     cudaGetDevice(&dev);
     if (configured_dev != dev) {
-        cudaError_t e = cudaFuncSetAttribute(os_pass_kernel<XP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(os_pass_kernel<XP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)axis_smem_limit());
         if (e != cudaSuccess) return e;
         configured_dev = dev;
     }
-    os_pass_kernel<XP><<<tiles, OS_NT, os_smem_bytes(rmin, XP ? PASS_X : PASS_Y), st>>>(jobs, njobs);
+    os_pass_kernel<XP, MINB><<<tiles, OS_NT, os_smem_bytes(rmin, XP ? PASS_X : PASS_Y), st>>>(jobs, njobs);
     note_launch();
     return cudaGetLastError();
 }
@@ -535,8 +555,12 @@ cudaError_t launch_os(const OsJob *jobs, int njobs, int tiles, int rmin, int axi
         ready = dev >= 0 && dev < 64 && g_tw_done[dev];
     }
     if (!ready && (e = os_prepare()) != cudaSuccess) return e;
-    if (axis == PASS_X) return launch_os_t<true>(jobs, njobs, tiles, rmin, st);
-    return launch_os_t<false>(jobs, njobs, tiles, rmin, st);
+    if (os_min_blocks() == 4) {
+        if (axis == PASS_X) return launch_os_t<true, 4>(jobs, njobs, tiles, rmin, st);
+        return launch_os_t<false, 4>(jobs, njobs, tiles, rmin, st);
+    }
+    if (axis == PASS_X) return launch_os_t<true, 3>(jobs, njobs, tiles, rmin, st);
+    return launch_os_t<false, 3>(jobs, njobs, tiles, rmin, st);
 }
 
 }  // namespace vfd
