@@ -212,47 +212,59 @@ __host__ __device__ inline OsGeom os_geom(int r, int C, bool xpass)
 // multiples of 4 (a 4-position quad then lies wholly inside or outside the
 // line).  y/z with vec: positions 16-byte aligned.
 template <bool XP>
-__device__ __forceinline__ void os_stage(float *stage, const OsJob &j, const OsGeom &G, const float *base,
-                                         int nreal, int pa, int sfirst, int send, bool vec)
+__device__ __forceinline__ void os_stage(float *stage, const OsJob &j, const float *base, int nreal, int pa,
+                                         int sfirst, int send, bool vec)
 {
     const int n = j.n;
     const int64_t ls = j.line_stride, ps = j.pos_stride;
     if (XP) {
         if (vec) {
+            // 8 threads per line row, 16 bytes (4 positions) each
             const int row = threadIdx.x >> 3, k = threadIdx.x & 7;
             const bool rok = row < nreal;
-            const float *src = base + (rok ? row : 0) * ls;
-            float *dst = stage + row * G.RS;
+            const float *src = base + (rok ? row : 0) * ls + pa;
+            float *dst = stage + row * j.RS;
+            if (rok && pa + sfirst >= 0 && pa + send <= n) {
 #pragma unroll 2
-            for (int s = sfirst + 4 * k; s < send; s += 32) {
-                const int p = pa + s;
-                const bool v = rok && p >= 0 && p < n;
-                cp_async16(dst + s, v ? src + p : base, v ? 16 : 0);
+                for (int s = sfirst + 4 * k; s < send; s += 32) cp_async16(dst + s, src + s, 16);
+            } else {
+#pragma unroll 2
+                for (int s = sfirst + 4 * k; s < send; s += 32) {
+                    const bool v = rok && (unsigned)(pa + s) < (unsigned)n;
+                    cp_async16(dst + s, v ? src + s : base, v ? 16 : 0);
+                }
             }
         } else {
             const int wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
             for (int row = wp; row < 32; row += OS_NT / 32) {
                 const bool rok = row < nreal;
-                const float *src = base + (rok ? row : 0) * ls;
-                float *dst = stage + row * G.RS;
+                const float *src = base + (rok ? row : 0) * ls + pa;
+                float *dst = stage + row * j.RS;
                 for (int s = sfirst + lane; s < send; s += 32) {
-                    const int p = pa + s;
-                    const bool v = rok && p >= 0 && p < n;
-                    cp_async4(dst + s, v ? src + p : base, v);
+                    const bool v = rok && (unsigned)(pa + s) < (unsigned)n;
+                    cp_async4(dst + s, v ? src + s : base, v);
                 }
             }
         }
     } else {
         if (vec) {
+            // 8 threads per position row, 16 bytes (4 lines) each
+            constexpr int STEP = OS_NT / 8;
             const int k = threadIdx.x & 7, sub = threadIdx.x >> 3;
             const int vb = 4 * min(max(nreal - 4 * k, 0), 4);
-            const float *src = base + 4 * k;
-            float *dst = stage + 4 * k;
+            int i = sfirst + sub;
+            const float *src = base + 4 * k + (int64_t)(pa + i) * ps;
+            float *dst = stage + i * OS_RS + 4 * k;
+            const int64_t gstep = STEP * ps;
+            if (vb == 16 && pa + sfirst >= 0 && pa + send <= n) {
 #pragma unroll 2
-            for (int i = sfirst + sub; i < send; i += OS_NT / 8) {
-                const int p = pa + i;
-                const bool v = vb > 0 && p >= 0 && p < n;
-                cp_async16(dst + i * OS_RS, v ? src + (int64_t)p * ps : base, v ? vb : 0);
+                for (; i < send; i += STEP, src += gstep, dst += STEP * OS_RS) cp_async16(dst, src, 16);
+            } else {
+#pragma unroll 2
+                for (; i < send; i += STEP, src += gstep, dst += STEP * OS_RS) {
+                    const bool v = vb > 0 && (unsigned)(pa + i) < (unsigned)n;
+                    cp_async16(dst, v ? src : base, v ? vb : 0);
+                }
             }
         } else {
             const int col = threadIdx.x & 31, wp = threadIdx.x >> 5;
@@ -260,178 +272,250 @@ __device__ __forceinline__ void os_stage(float *stage, const OsJob &j, const OsG
             const float *src = base + (cok ? col : 0) * ls;
             for (int i = sfirst + wp; i < send; i += OS_NT / 32) {
                 const int p = pa + i;
-                const bool v = cok && p >= 0 && p < n;
+                const bool v = cok && (unsigned)p < (unsigned)n;
                 cp_async4(stage + i * OS_RS + col, v ? src + (int64_t)p * ps : base, v);
             }
         }
     }
 }
 
+// Staging slots a chunk of nb blocks reads.
+__device__ __forceinline__ int os_slots(const OsJob &J, int nb, bool xpass)
+{
+    return xpass ? ((J.delta + nb * J.L + 2 * J.r + 3) & ~3) : nb * J.L + 2 * J.r;
+}
+
+__device__ __forceinline__ float *os_tile_base(const OsJob &J, const OsTileInfo &T)
+{
+    return J.data + T.outer * J.outer_stride + (int64_t)T.l0 * J.line_stride;
+}
+
+// Persistent pass: CTA c takes tiles c, c + grid, c + 2 grid, ... and walks
+// their chunks as one stream of steps.  At the top of each step the next
+// step's input is requested (the next chunk of this tile, or the first chunk
+// of the next tile), so a tile's first load overlaps the previous tile's last
+// chunk.  Tile records and job descriptors live in a ring of three shared
+// slots (the CTA's k-th tile in slot k % 3); warp 0 fetches tile k + 2's
+// during tile k's first step, when slot (k + 2) % 3 = (k - 1) % 3 is free.
+// Mass partial sums are flushed per warp (warp reduction, one atomic per
+// value) whenever the job changes.
 template <bool XP, int MINB>
-__global__ void __launch_bounds__(OS_NT, MINB) os_pass_kernel(const OsJob *__restrict__ jobs, int njobs)
+__global__ void __launch_bounds__(OS_NT, MINB)
+    os_pass_kernel(const OsJob *__restrict__ jobs, const OsTileInfo *__restrict__ tiles, int ntiles, int stage_floats)
 {
     extern __shared__ __align__(16) float osm[];
-    __shared__ double red[OS_NT / 32];
-    __shared__ __align__(16) OsJob sj;
-    __shared__ __align__(16) float2 hh[OS_N];  // (H[k], H[k]) for packed scaling
-    __shared__ int sjob;
+    __shared__ __align__(16) OsJob sj[3];
+    __shared__ __align__(16) OsTileInfo st[3];
 
-    // ---- job descriptor: found by one lane, copied by its warp -------------
-    const int tile = blockIdx.x;
-    if (threadIdx.x < 32) {
-        if (threadIdx.x == 0) {
-            int lo = 0, hi = njobs - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (jobs[mid].tile_begin <= tile) lo = mid;
-                else hi = mid - 1;
-            }
-            sjob = lo;
-        }
-        __syncwarp();
-        const int *src = reinterpret_cast<const int *>(jobs + sjob);
-        int *dst = reinterpret_cast<int *>(&sj);
-        for (int i = threadIdx.x; i < (int)(sizeof(OsJob) / sizeof(int)); i += 32) dst[i] = src[i];
+    const int grid = gridDim.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int tile = blockIdx.x;
+    if (tile >= ntiles) return;
+
+    // warp 0: tile record and job descriptor of a tile into a slot
+    auto fetch = [&](int slot, const OsTileInfo &ti) {
+        if (lane == 0) st[slot] = ti;
+        const float *src = reinterpret_cast<const float *>(jobs + ti.job);
+        float *dst = reinterpret_cast<float *>(&sj[slot]);
+        for (int i = lane; i < (int)(sizeof(OsJob) / 16); i += 32) cp_async16(dst + 4 * i, src + 4 * i, 16);
+    };
+    if (warp == 0) {
+        fetch(0, tiles[tile]);
+        if (tile + grid < ntiles) fetch(1, tiles[tile + grid]);
+        cp_async_commit();
     }
+    cp_async_wait_all();
     __syncthreads();
-    if (threadIdx.x < OS_N) hh[threadIdx.x] = make_float2(sj.H[threadIdx.x], sj.H[threadIdx.x]);
 
-    const int n = sj.n, r = sj.r, L = sj.L, C = sj.C;
-    const OsGeom G = os_geom(r, C, XP);
-    const int hs = r + G.delta;  // slots a chunk carries over from the previous one (x: a multiple of 4)
-
-    const int local = tile - sj.tile_begin;
-    const int outer = local / sj.tiles_per_outer;
-    const int l0 = (local - outer * sj.tiles_per_outer) * 32;
-    const int nreal = min(32, sj.nlines - l0);
-    float *const base = sj.data + outer * sj.outer_stride + (int64_t)l0 * sj.line_stride;
-    const int64_t ls = sj.line_stride, ps = sj.pos_stride;
-    const int nch = sj.nchunks, nblocks = sj.nblocks, ofirst = sj.ofirst;
-    const bool aligned = (reinterpret_cast<uintptr_t>(base) & 15) == 0;
-    const bool vec = XP ? (aligned && (ls & 3) == 0 && (n & 3) == 0 && (ofirst & 3) == 0)
-                        : (aligned && ls == 1 && (ps & 3) == 0);
-
-    // ---- per-lane constants of the FFT phase: group g = (pair, block) ------
+    // ---- per-lane constants: group g = (pair, block) ----------------------
     // The 4 groups of a warp share the block, so block-uniform branches are
     // warp-uniform (fft64_* synchronise the whole warp).
     const int g = threadIdx.x >> 3, t = threadIdx.x & 7;
-    const int pair = g & 15, blk = g >> 4, seg0 = blk * L;
-    float2 *const gs = reinterpret_cast<float2 *>(osm + 2 * G.stage) + g * OS_SCR;
+    const int pair = g & 15, blk = g >> 4;
+    float2 *const gs = reinterpret_cast<float2 *>(osm + 2 * stage_floats) + g * OS_SCR;
     float2 *const wr = gs + t;
     const float2 *const rd = gs + 9 * t;
     float2 w[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) w[k] = c_tw64[(t * k) & 63];
-    unsigned qmask = 0;  // samples t + 8q that are outputs of the block
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const int i = t + 8 * q;
-        if (i >= r && i < r + L) qmask |= 1u << q;
-    }
-    const bool va = 2 * pair < nreal, vb = 2 * pair + 1 < nreal;  // real lines of this pair
-    // y/z outputs of a pair go out as one 8-byte store when aligned
-    const bool st2 = !XP && vb && ((reinterpret_cast<uintptr_t>(base) & 7) == 0) && ((ps & 1) == 0);
-    // constant-VF padding rule (x pass): rows of this pair inside the y/z box
-    const bool masked = XP && sj.mask;
-    const float b = sj.b;
-    bool in_a = false, in_b = false;
-    if (masked) {
-        if (va) {
-            const int rr = l0 + 2 * pair, y = rr % sj.ny, z = rr / sj.ny;
-            in_a = y >= sj.box_lo[1] && y < sj.box_hi[1] && z >= sj.box_lo[2] && z < sj.box_hi[2];
-        }
-        if (vb) {
-            const int rr = l0 + 2 * pair + 1, y = rr % sj.ny, z = rr / sj.ny;
-            in_b = y >= sj.box_lo[1] && y < sj.box_hi[1] && z >= sj.box_lo[2] && z < sj.box_hi[2];
-        }
-    }
-    const bool zlast = !XP && sj.kind == PASS_Z;
-    const float2 keep2 = make_float2(sj.keep, sj.keep), b2 = make_float2(b, b);
 
-    // staging slots a chunk of nb blocks needs
-    auto slots = [&](int nb) { return XP ? ((G.delta + nb * L + 2 * r + 3) & ~3) : nb * L + 2 * r; };
-
-    os_stage<XP>(osm, sj, G, base, nreal, ofirst - r - G.delta, 0, slots(min(OS_M, nblocks)), vec);
-    cp_async_commit();
+    // first step: chunk 0 of the first tile
+    {
+        const OsJob &J = sj[0];
+        const OsTileInfo T = st[0];
+        os_stage<XP>(osm, J, os_tile_base(J, T), T.flags & 63, J.ofirst - J.r - J.delta, 0,
+                     os_slots(J, min(OS_M, J.nblocks), XP), (T.flags >> 8) & 1);
+        cp_async_commit();
+    }
 
     double acc_in = 0.0, acc_leak = 0.0, acc_conv = 0.0, acc_out = 0.0;
-    for (int ch = 0; ch < nch; ++ch) {
-        const int c0 = ofirst + ch * C, p0 = c0 - r;
-        const int nb = min(OS_M, nblocks - ch * OS_M);
-        float *const in = osm + (ch & 1) * G.stage;
-        float *const nxt = osm + ((ch & 1) ^ 1) * G.stage;
-        // chunk ch has landed (copies and carried slots), and every thread is
-        // done with the previous chunk (its reads of `nxt`)
+    auto flush = [&](const OsJob &J) {
+        double *mass = J.mass;
+        const double a0 = os_warp_sum(acc_in), a1 = os_warp_sum(acc_leak);
+        const double a2 = os_warp_sum(acc_conv), a3 = os_warp_sum(acc_out);
+        if (lane == 0) {
+            if (XP) {
+                if (a0 != 0.0) atomicAdd(mass + MS_INPUT, a0);
+                if (a1 != 0.0) atomicAdd(mass + MS_LEAK_X, a1);
+            } else if (J.kind == PASS_Y) {
+                if (a1 != 0.0) atomicAdd(mass + MS_LEAK_Y, a1);
+            } else {
+                if (a1 != 0.0) atomicAdd(mass + MS_LEAK_Z, a1);
+                if (a2 != 0.0) atomicAdd(mass + MS_CONV, a2);
+                if (a3 != 0.0) atomicAdd(mass + MS_OUT, a3);
+            }
+        }
+        acc_in = acc_leak = acc_conv = acc_out = 0.0;
+    };
+
+    int slot = 0, ch = 0, buf = 0;
+    for (;;) {
+        const OsJob &J = sj[slot];
+        const int slot1 = slot == 2 ? 0 : slot + 1, slot2 = slot1 == 2 ? 0 : slot1 + 1;
+        // this step's input has landed (copies and carried slots), every
+        // thread is done with the previous step, and records fetched during
+        // the previous step are visible
         cp_async_wait_all();
         __syncthreads();
-        if (ch + 1 < nch) {
-            // next chunk, slots [hs, ..): positions >= c0 + C, which this
-            // chunk does not store
-            os_stage<XP>(nxt, sj, G, base, nreal, p0 + C - G.delta, hs, slots(min(OS_M, nblocks - (ch + 1) * OS_M)),
-                         vec);
+        // warp 0: record of the CTA's tile after next (fetched after the FFT phase)
+        OsTileInfo ti2;
+        ti2.job = -1;
+        if (warp == 0 && ch == 0 && tile + 2 * grid < ntiles) ti2 = tiles[tile + 2 * grid];
+
+        const OsTileInfo T = st[slot];
+        float *const base = os_tile_base(J, T);
+        const int nreal = T.flags & 63;
+        const int r = J.r, L = J.L, C = J.C, n = J.n;
+        const int c0 = J.ofirst + ch * C, p0 = c0 - r;
+        const int nb = min(OS_M, J.nblocks - ch * OS_M);
+        float *const in = osm + buf * stage_floats;
+        float *const nxt = osm + (buf ^ 1) * stage_floats;
+        const bool same = ch + 1 < J.nchunks;
+        const bool has_next = same || tile + grid < ntiles;
+
+        // ---- request the next step's input ---------------------------------
+        if (same) {
+            // this tile's next chunk, slots [hs, ..): positions >= c0 + C,
+            // which this step does not store
+            const int hs = J.hs;
+            os_stage<XP>(nxt, J, base, nreal, p0 + C - J.delta, hs, os_slots(J, min(OS_M, J.nblocks - (ch + 1) * OS_M), XP),
+                         (T.flags >> 8) & 1);
             cp_async_commit();
-            // slots [0, hs): inputs this chunk overwrites, carried in shared memory
+            // slots [0, hs): inputs this step overwrites, carried in shared memory
             if (XP) {
-                const int q4 = hs >> 2;
-                for (int i = threadIdx.x; i < 32 * q4; i += OS_NT) {
-                    const int row = i / q4, c = i - row * q4;
-                    reinterpret_cast<float4 *>(nxt + row * G.RS)[c] =
-                        reinterpret_cast<const float4 *>(in + row * G.RS + C)[c];
-                }
+                const int row = threadIdx.x >> 3, c = threadIdx.x & 7;  // hs <= 16: 4 float4 per row
+                if (4 * c < hs)
+                    reinterpret_cast<float4 *>(nxt + row * J.RS)[c] =
+                        reinterpret_cast<const float4 *>(in + row * J.RS + C)[c];
             } else {
                 const float4 *hsrc = reinterpret_cast<const float4 *>(in + C * OS_RS);
                 float4 *hdst = reinterpret_cast<float4 *>(nxt);
                 for (int i = threadIdx.x; i < hs * (OS_RS / 4); i += OS_NT) hdst[i] = hsrc[i];
             }
+        } else if (has_next) {
+            // first chunk of the next tile (other lines: no overlap with this step's stores)
+            const OsJob &Jn = sj[slot1];
+            const OsTileInfo Tn = st[slot1];
+            os_stage<XP>(nxt, Jn, os_tile_base(Jn, Tn), Tn.flags & 63, Jn.ofirst - Jn.r - Jn.delta, 0,
+                         os_slots(Jn, min(OS_M, Jn.nblocks), XP), (Tn.flags >> 8) & 1);
+            cp_async_commit();
         }
 
         // ---- one block of one pair per group: FFT-64, multiply, inverse,
         // outputs straight to global memory -------------------------------
+        const int seg0 = blk * L;
         if (blk < nb) {
+            const int64_t ls = J.line_stride, ps = J.pos_stride;
+            const float b = J.b;
+            const bool va = 2 * pair < nreal, vb = 2 * pair + 1 < nreal;  // real lines of this pair
+            const unsigned qmask = J.qmask[t];  // samples t + 8q that are outputs of the block
             float2 x[8];
             if (XP) {
-                const float *ra = in + (2 * pair) * G.RS + G.delta + seg0 + t;
-                const float *rb = ra + G.RS;
+                const float *ra = in + (2 * pair) * J.RS + J.delta + seg0 + t;
+                const float *rb = ra + J.RS;
 #pragma unroll
                 for (int q = 0; q < 8; ++q) x[q] = make_float2(ra[8 * q], rb[8 * q]);
-            } else {
-                const float2 *sp = reinterpret_cast<const float2 *>(in + (seg0 + t) * OS_RS) + pair;
+                if (J.mask) {
+                    // constant-VF padding rule: rows inside the y/z box, positions inside [lo, hi)
+                    bool in_a = false, in_b = false;
+                    if (va) {
+                        const int rr = T.l0 + 2 * pair, y = rr % J.ny, z = rr / J.ny;
+                        in_a = y >= J.box_lo[1] && y < J.box_hi[1] && z >= J.box_lo[2] && z < J.box_hi[2];
+                    }
+                    if (vb) {
+                        const int rr = T.l0 + 2 * pair + 1, y = rr % J.ny, z = rr / J.ny;
+                        in_b = y >= J.box_lo[1] && y < J.box_hi[1] && z >= J.box_lo[2] && z < J.box_hi[2];
+                    }
 #pragma unroll
-                for (int q = 0; q < 8; ++q) x[q] = sp[q * 8 * (OS_RS / 2)];
-            }
-            if (masked) {
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const int p = p0 + seg0 + t + 8 * q;
-                    const bool px = p >= sj.box_lo[0] && p < sj.box_hi[0];
-                    x[q].x = (in_a && px) ? x[q].x - b : 0.0f;
-                    x[q].y = (in_b && px) ? x[q].y - b : 0.0f;
+                    for (int q = 0; q < 8; ++q) {
+                        const int p = p0 + seg0 + t + 8 * q;
+                        const bool px = p >= J.box_lo[0] && p < J.box_hi[0];
+                        x[q].x = (in_a && px) ? x[q].x - b : 0.0f;
+                        x[q].y = (in_b && px) ? x[q].y - b : 0.0f;
+                    }
                 }
-            }
-            if (XP) {
                 // input mass: each position of a line is one block's output once
                 float2 s2 = make_float2(0.0f, 0.0f);
 #pragma unroll
                 for (int q = 0; q < 8; ++q)
                     if ((qmask >> q) & 1u) s2 = p_add(s2, x[q]);
                 acc_in += (double)((va ? s2.x : 0.0f) + (vb ? s2.y : 0.0f));
+            } else {
+                const float2 *sp = reinterpret_cast<const float2 *>(in + (seg0 + t) * OS_RS) + pair;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) x[q] = sp[q * 8 * (OS_RS / 2)];
             }
             fft64_fwd(x, wr, rd, w);
 #pragma unroll
-            for (int k = 0; k < 8; ++k) x[k] = p_mul(x[k], hh[t + 8 * k]);
+            for (int q = 0; q < 8; ++q) x[q] = p_mul(x[q], J.HH[t + 8 * q]);
             fft64_inv(x, wr, rd, w);
 
             const int ob = c0 + seg0 + t - r;  // position of sample t (q = 0)
             const bool inside = c0 + seg0 >= 0 && c0 + seg0 + L <= n;
+            const bool zlast = !XP && J.kind == PASS_Z;
+            // y/z outputs of a pair go out as one 8-byte store when aligned
+            const bool st2 = !XP && vb && ((reinterpret_cast<uintptr_t>(base) & 7) == 0) && ((ps & 1) == 0);
+            const float2 keep2 = make_float2(J.keep, J.keep), b2 = make_float2(b, b);
             float2 lk2 = make_float2(0.0f, 0.0f), cv2 = lk2, ot2 = lk2;
-            if (XP) {
+            if (inside) {
+                // every kept sample is stored: addresses are a base plus constants
+                if (XP) {
+                    float *da = base + (2 * pair) * ls + ob;
+                    float *db = da + ls;
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        if (!((qmask >> q) & 1u)) continue;
+                        if (va) da[8 * q] = x[q].x;
+                        if (vb) db[8 * q] = x[q].y;
+                    }
+                } else {
+                    float *d = base + 2 * pair + (int64_t)ob * ps;
+                    const int64_t step = 8 * ps;
+#pragma unroll
+                    for (int q = 0; q < 8; ++q, d += step) {
+                        if (!((qmask >> q) & 1u)) continue;
+                        float2 v = x[q];
+                        if (zlast) {
+                            cv2 = p_add(cv2, v);
+                            v = p_mul(p_add(v, b2), keep2);
+                            ot2 = p_add(ot2, v);
+                        }
+                        if (st2) {
+                            *reinterpret_cast<float2 *>(d) = v;
+                        } else {
+                            if (va) d[0] = v.x;
+                            if (vb) d[1] = v.y;
+                        }
+                    }
+                }
+            } else if (XP) {
                 float *da = base + (2 * pair) * ls;
                 float *db = da + ls;
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
                     if (!((qmask >> q) & 1u)) continue;
                     const int o = ob + 8 * q;
-                    if (inside || (o >= 0 && o < n)) {
+                    if (o >= 0 && o < n) {
                         if (va) da[o] = x[q].x;
                         if (vb) db[o] = x[q].y;
                     } else if (o >= -r && o < n + r) {
@@ -439,13 +523,12 @@ __global__ void __launch_bounds__(OS_NT, MINB) os_pass_kernel(const OsJob *__res
                     }
                 }
             } else {
-                float *d = base + 2 * pair + (int64_t)ob * ps;
-                const int64_t step = 8 * ps;
 #pragma unroll
-                for (int q = 0; q < 8; ++q, d += step) {
+                for (int q = 0; q < 8; ++q) {
                     if (!((qmask >> q) & 1u)) continue;
                     const int o = ob + 8 * q;
-                    if (inside || (o >= 0 && o < n)) {
+                    if (o >= 0 && o < n) {
+                        float *d = base + 2 * pair + (int64_t)o * ps;
                         float2 v = x[q];
                         if (zlast) {
                             cv2 = p_add(cv2, v);
@@ -469,19 +552,61 @@ __global__ void __launch_bounds__(OS_NT, MINB) os_pass_kernel(const OsJob *__res
                 acc_out += (double)((va ? ot2.x : 0.0f) + (vb ? ot2.y : 0.0f));
             }
         }
-    }
 
-    double *mass = sj.mass;
-    if (XP) {
-        os_block_sum(acc_in, mass + MS_INPUT, red);
-        os_block_sum(acc_leak, mass + MS_LEAK_X, red);
-    } else if (sj.kind == PASS_Y) {
-        os_block_sum(acc_leak, mass + MS_LEAK_Y, red);
-    } else {
-        os_block_sum(acc_leak, mass + MS_LEAK_Z, red);
-        os_block_sum(acc_conv, mass + MS_CONV, red);
-        os_block_sum(acc_out, mass + MS_OUT, red);
+        if (ti2.job >= 0) {  // warp 0: the tile after next into the free slot
+            fetch(slot2, ti2);
+            cp_async_commit();
+        }
+        if (!has_next) {
+            flush(J);
+            break;
+        }
+        if (same) {
+            ++ch;
+        } else {
+            if (sj[slot1].mass != J.mass) flush(J);
+            slot = slot1;
+            tile += grid;
+            ch = 0;
+        }
+        buf ^= 1;
     }
+}
+
+void os_finish_job(OsJob &j)
+{
+    const OsGeom g = os_geom(j.r, j.C, j.kind == PASS_X);
+    j.delta = g.delta;
+    j.RS = g.RS;
+    j.hs = j.r + g.delta;
+    for (int t = 0; t < 8; ++t) {
+        unsigned m = 0;
+        for (int q = 0; q < 8; ++q) {
+            const int i = t + 8 * q;
+            if (i >= j.r && i < j.r + j.L) m |= 1u << q;
+        }
+        j.qmask[t] = (unsigned char)m;
+    }
+}
+
+void os_append_tiles(const OsJob &j, int job, std::vector<OsTileInfo> &out)
+{
+    const bool xpass = j.kind == PASS_X;
+    for (int outer = 0; outer < j.nouter; ++outer)
+        for (int lt = 0; lt < j.tiles_per_outer; ++lt) {
+            OsTileInfo ti;
+            ti.job = job;
+            ti.outer = outer;
+            ti.l0 = lt * 32;
+            const int nreal = std::min(32, j.nlines - ti.l0);
+            const uintptr_t base = reinterpret_cast<uintptr_t>(j.data) +
+                                   sizeof(float) * (uintptr_t)(outer * j.outer_stride + (int64_t)ti.l0 * j.line_stride);
+            const bool aligned = (base & 15) == 0;
+            const bool vec = xpass ? (aligned && (j.line_stride & 3) == 0 && (j.n & 3) == 0 && (j.ofirst & 3) == 0)
+                                   : (aligned && j.line_stride == 1 && (j.pos_stride & 3) == 0);
+            ti.flags = nreal | (vec ? 1 << 8 : 0);
+            out.push_back(ti);
+        }
 }
 
 static std::mutex g_tw_mu;
@@ -527,25 +652,44 @@ static int os_min_blocks()
 }
 
 template <bool XP, int MINB>
-static cudaError_t launch_os_t(const OsJob *jobs, int njobs, int tiles, int rmin, cudaStream_t st)
+static cudaError_t launch_os_t(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int rmin, cudaStream_t st)
 {
-    static thread_local int configured_dev = -1;
+    static std::mutex mu;
+    static int configured[64] = {};  // 1 + resident CTAs per SM at the configured size
+    static size_t configured_smem[64] = {};
     int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_dev != dev) {
-        cudaError_t e = cudaFuncSetAttribute(os_pass_kernel<XP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)axis_smem_limit());
-        if (e != cudaSuccess) return e;
-        configured_dev = dev;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    const size_t smem = os_smem_bytes(rmin, XP ? PASS_X : PASS_Y);
+    int per_sm = 0, nsm = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (configured[dev] == 0 || configured_smem[dev] != smem) {
+            e = cudaFuncSetAttribute(os_pass_kernel<XP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)axis_smem_limit());
+            if (e != cudaSuccess) return e;
+            int b = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, os_pass_kernel<XP, MINB>, OS_NT, smem);
+            if (e != cudaSuccess) return e;
+            configured[dev] = 1 + std::max(b, 1);
+            configured_smem[dev] = smem;
+        }
+        per_sm = configured[dev] - 1;
     }
-    os_pass_kernel<XP, MINB><<<tiles, OS_NT, os_smem_bytes(rmin, XP ? PASS_X : PASS_Y), st>>>(jobs, njobs);
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    const int grid = std::min(ntiles, per_sm * nsm);
+    int stage_floats = 0;
+    for (int r = std::max(rmin, 0); r <= OS_RMAX; ++r)
+        stage_floats = std::max(stage_floats, os_geom(r, OS_M * (OS_N - 2 * r), XP).stage);
+    os_pass_kernel<XP, MINB><<<grid, OS_NT, smem, st>>>(jobs, tiles, ntiles, stage_floats);
     note_launch();
     return cudaGetLastError();
 }
 
-cudaError_t launch_os(const OsJob *jobs, int njobs, int tiles, int rmin, int axis, cudaStream_t st)
+cudaError_t launch_os(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int rmin, int axis, cudaStream_t st)
 {
-    if (tiles <= 0) return cudaSuccess;
+    if (ntiles <= 0) return cudaSuccess;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -556,11 +700,11 @@ cudaError_t launch_os(const OsJob *jobs, int njobs, int tiles, int rmin, int axi
     }
     if (!ready && (e = os_prepare()) != cudaSuccess) return e;
     if (os_min_blocks() == 4) {
-        if (axis == PASS_X) return launch_os_t<true, 4>(jobs, njobs, tiles, rmin, st);
-        return launch_os_t<false, 4>(jobs, njobs, tiles, rmin, st);
+        if (axis == PASS_X) return launch_os_t<true, 4>(jobs, tiles, ntiles, rmin, st);
+        return launch_os_t<false, 4>(jobs, tiles, ntiles, rmin, st);
     }
-    if (axis == PASS_X) return launch_os_t<true, 3>(jobs, njobs, tiles, rmin, st);
-    return launch_os_t<false, 3>(jobs, njobs, tiles, rmin, st);
+    if (axis == PASS_X) return launch_os_t<true, 3>(jobs, tiles, ntiles, rmin, st);
+    return launch_os_t<false, 3>(jobs, tiles, ntiles, rmin, st);
 }
 
 }  // namespace vfd

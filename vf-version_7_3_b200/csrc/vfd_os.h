@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "vfd_axis.cuh"
 
 namespace vfd {
@@ -13,7 +15,7 @@ constexpr int OS_M = 2;       // blocks per chunk
 
 // One (field, axis) pass; line addressing as in AxisJob.  A tile is 32 real
 // lines of one outer index over their whole length (all chunks, in order).
-struct OsJob {
+struct alignas(16) OsJob {
     float *data;
     double *mass;
     int64_t line_stride, outer_stride, pos_stride;
@@ -30,18 +32,38 @@ struct OsJob {
     float b, keep;
     int nx, ny;
     int box_lo[3], box_hi[3];
-    float H[OS_N];         // G64(k) / 64, FP64-generated
+    // shared-memory geometry (host-computed, see os_geom in vfd_os.cu)
+    int delta;             // x pass: staged window starts delta positions before a chunk's first input
+    int RS;                // x pass: floats per staged line row
+    int hs;                // staging slots carried from one chunk to the next: r + delta
+    unsigned char qmask[8];  // lane t of a group: bit q set when sample t + 8q is a block output
+    float2 HH[OS_N];       // (G64(k) / 64) twice, FP64-generated
 };
+static_assert(sizeof(OsJob) % 16 == 0, "OsJob is copied in 16-byte pieces");
 
 // First output position of chunk 0 for a pass of radius r along `axis`.
 inline int os_first_output(int r, int axis) { return axis == PASS_X ? -(r + ((-r) & 3)) : -r; }
+
+// A tile of a persistent launch: its job, position and lines.
+struct OsTileInfo {
+    int job;    // index into the launch's job array
+    int outer;  // outer index of the tile's lines
+    int l0;     // first line within the outer index
+    int flags;  // bits 0-5: real lines (1..32); bit 8: 16-byte copies apply
+};
+
+// Fills the host-computed geometry fields of a job whose other fields are set.
+void os_finish_job(OsJob &j);
+// Appends the tiles of job `job` (j) to `out`.
+void os_append_tiles(const OsJob &j, int job, std::vector<OsTileInfo> &out);
 
 // Uploads the FFT-64 twiddles to the current device; call outside any stream
 // capture before the first launch on a device (world and batch creation do).
 cudaError_t os_prepare();
 // Dynamic shared memory of a launch whose jobs have radius >= rmin.
 size_t os_smem_bytes(int rmin, int axis);
-// All jobs of a launch belong to `axis`.
-cudaError_t launch_os(const OsJob *jobs, int njobs, int tiles, int rmin, int axis, cudaStream_t st);
+// One persistent launch over `ntiles` tiles (tiles[i]) of jobs that all
+// belong to `axis` and have radius >= rmin.
+cudaError_t launch_os(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int rmin, int axis, cudaStream_t st);
 
 }  // namespace vfd

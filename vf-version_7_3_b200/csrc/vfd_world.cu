@@ -203,6 +203,8 @@ struct vfd_world {
     int rmin[3] = {0, 0, 0};
     OsJob *d_osjobs = nullptr;             // [pass][nf] all-field, then [pass][nf] single-field
     std::vector<int> os_tiles[3];          // per field
+    OsTileInfo *d_os_tiles[3] = {nullptr, nullptr, nullptr};    // all-field launches
+    OsTileInfo *d_os_ftiles[3] = {nullptr, nullptr, nullptr};   // single-field launches, [field][tiles]
 
     float *d_fields = nullptr;
     float2 *d_tw[3] = {nullptr, nullptr, nullptr};
@@ -277,6 +279,10 @@ static void release(vfd_world *w)
     cudaFree(w->d_mass);
     cudaFree(w->d_jobs);
     cudaFree(w->d_osjobs);
+    for (int a = 0; a < 3; ++a) {
+        cudaFree(w->d_os_tiles[a]);
+        cudaFree(w->d_os_ftiles[a]);
+    }
     cudaFree(w->d_err);
     cudaFree(w->d_src_idx);
     cudaFree(w->d_src_amt);
@@ -372,6 +378,15 @@ static bool os_enabled()
 
 static bool os_plain_staging(const OsJob &j);
 
+// Copies v to a new device array (at least one element).
+template <class T>
+static cudaError_t upload_vec(T **d, const std::vector<T> &v)
+{
+    cudaError_t e = cudaMalloc(d, sizeof(T) * std::max<size_t>(v.size(), 1));
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpy(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+}
+
 static OsJob make_os_job(const vfd_world *w, int f, int a, int tile_begin)
 {
     const AxisJob aj = make_job(w, f, a, 0, 16);
@@ -403,9 +418,10 @@ static OsJob make_os_job(const vfd_world *w, int f, int a, int tile_begin)
         j.box_hi[i] = aj.box_hi[i];
     }
     j.mask = os_plain_staging(j) ? 0 : 1;
+    os_finish_job(j);
     std::vector<float> h;
     gauss_spectrum(w->params[f].sigma[a], j.r, OS_N, h);
-    for (int k = 0; k < OS_N; ++k) j.H[k] = h[k];
+    for (int k = 0; k < OS_N; ++k) j.HH[k] = make_float2(h[k], h[k]);
     return j;
 }
 
@@ -612,6 +628,16 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
         if ((e = cudaMalloc(&w->d_osjobs, sizeof(OsJob) * oj.size())) != cudaSuccess) return bail(e, "cudaMalloc os jobs");
         if ((e = cudaMemcpy(w->d_osjobs, oj.data(), sizeof(OsJob) * oj.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
             return bail(e, "cudaMemcpy os jobs");
+        for (int a = 0; a < 3; ++a) {
+            std::vector<OsTileInfo> all, one;
+            for (int f = 0; f < w->nf; ++f) {
+                os_append_tiles(oj[(size_t)a * w->nf + f], f, all);
+                os_append_tiles(oj[(size_t)(3 + a) * w->nf + f], 0, one);
+            }
+            if ((e = upload_vec(&w->d_os_tiles[a], all)) != cudaSuccess ||
+                (e = upload_vec(&w->d_os_ftiles[a], one)) != cudaSuccess)
+                return bail(e, "os tiles");
+        }
     }
     if ((e = cudaMalloc(&w->d_dep, sizeof(DepositJob) * 2 * w->nf)) != cudaSuccess) return bail(e, "cudaMalloc deposit jobs");
     if (general) {
@@ -1068,7 +1094,12 @@ static vfd_status enqueue_tick(vfd_world *w, int field, int n_substeps, cudaStre
                     for (int f = 0; f < w->nf; ++f) tiles += w->os_tiles[a][f];
                 else
                     tiles = w->os_tiles[a][field];
-                VFD_CUDA(w, launch_os(jobs, nj, tiles, w->rmin[a], a, st));
+                const OsTileInfo *ti = w->d_os_tiles[a];
+                if (field >= 0) {
+                    ti = w->d_os_ftiles[a];
+                    for (int f = 0; f < field; ++f) ti += w->os_tiles[a][f];
+                }
+                VFD_CUDA(w, launch_os(jobs, ti, tiles, w->rmin[a], a, st));
             } else {
                 const AxisJob *jobs = field < 0 ? w->d_jobs + a * w->nf : w->d_jobs + 3 * w->nf + a * w->nf + field;
                 const int tiles = w->tiles_per_field[a] * nj;
@@ -1237,6 +1268,7 @@ struct vfd_batch {
     int rmin[3] = {0, 0, 0};
     OsJob *d_osjobs = nullptr;  // [3][njobs]
     int os_tiles[3] = {0, 0, 0};
+    OsTileInfo *d_os_tiles[3] = {nullptr, nullptr, nullptr};
     cudaStream_t st = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     cudaGraph_t graph = nullptr;
@@ -1272,6 +1304,7 @@ static void batch_release(vfd_batch *b)
     if (b->graph) cudaGraphDestroy(b->graph);
     cudaFree(b->d_jobs);
     cudaFree(b->d_osjobs);
+    for (int a = 0; a < 3; ++a) cudaFree(b->d_os_tiles[a]);
     if (b->ev_in) cudaEventDestroy(b->ev_in);
     if (b->ev_out) cudaEventDestroy(b->ev_out);
     if (b->st) cudaStreamDestroy(b->st);
@@ -1320,6 +1353,7 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
     }
     b->njobs = (int)jobs.size() / 3;
     std::vector<OsJob> oj;
+    std::vector<OsTileInfo> tile_info[3];
     for (int a = 0; a < 3; ++a) {
         bool all = true;
         int rmn = 1 << 30;
@@ -1336,6 +1370,7 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
             for (auto *w : b->worlds)
                 for (int f = 0; f < w->nf; ++f) {
                     oj.push_back(make_os_job(w, f, a, tb));
+                    os_append_tiles(oj.back(), (int)(oj.size() - 1 - (size_t)a * b->njobs), tile_info[a]);
                     tb += os_field_tiles(oj.back());
                 }
             b->os_tiles[a] = tb;
@@ -1346,7 +1381,10 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
         cudaError_t e2 = cudaSuccess;
         if ((e2 = os_prepare()) != cudaSuccess ||
             (e2 = cudaMalloc(&b->d_osjobs, sizeof(OsJob) * oj.size())) != cudaSuccess ||
-            (e2 = cudaMemcpy(b->d_osjobs, oj.data(), sizeof(OsJob) * oj.size(), cudaMemcpyHostToDevice)) != cudaSuccess) {
+            (e2 = cudaMemcpy(b->d_osjobs, oj.data(), sizeof(OsJob) * oj.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e2 = upload_vec(&b->d_os_tiles[0], tile_info[0])) != cudaSuccess ||
+            (e2 = upload_vec(&b->d_os_tiles[1], tile_info[1])) != cudaSuccess ||
+            (e2 = upload_vec(&b->d_os_tiles[2], tile_info[2])) != cudaSuccess) {
             std::string msg = std::string("batch os jobs: ") + cudaGetErrorString(e2);
             batch_release(b);
             delete b;
@@ -1384,7 +1422,8 @@ static vfd_status batch_enqueue(vfd_batch *b, int n_substeps)
             VFD_BCUDA(b, cudaMemsetAsync(w->d_mass, 0, sizeof(double) * MS_COUNT * w->nf, b->st));
         for (int a = 0; a < 3; ++a) {
             if (b->use_os[a])
-                VFD_BCUDA(b, launch_os(b->d_osjobs + a * b->njobs, b->njobs, b->os_tiles[a], b->rmin[a], a, b->st));
+                VFD_BCUDA(b, launch_os(b->d_osjobs + a * b->njobs, b->d_os_tiles[a], b->os_tiles[a], b->rmin[a], a,
+                                       b->st));
             else
                 VFD_BCUDA(b, launch_axis(b->variant[a], b->d_jobs + a * b->njobs, b->njobs, b->tiles[a],
                                          b->Fmax[a], b->st));
