@@ -445,7 +445,7 @@ def main():
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": AXIS_TRAFFIC_BYTES,
-                "kernel": "os4_pass_kernel (x, y, z axis passes)",
+                "kernel": "os_pass_kernel (x, y, z axis passes)",
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
                 "peak_source": f"{peak_kind} hbm_gbs",
                 "share_of_step": axis_ms / ms if ms > 0 else None,

@@ -141,7 +141,7 @@ __device__ __forceinline__ void dft8p(float2 (&v)[8])
 // rows of 9 float2; lane t writes column t (wr = scr + t) and reads row t
 // (rd = scr + 9t), so every access is a base plus a constant offset.  All 32
 // lanes of the warp call it together (__syncwarp).
-__device__ __forceinline__ void fft64_fwd(float2 (&x)[8], float2 *wr, const float2 *rd, const float2 (&w)[8])
+__device__ __forceinline__ void fft64_fwd(float2 (&x)[8], float2 *wr, const float2 *rd, const float2 *w)
 {
     dft8p<false>(x);
 #pragma unroll
@@ -157,7 +157,7 @@ __device__ __forceinline__ void fft64_fwd(float2 (&x)[8], float2 *wr, const floa
 
 // Inverse of fft64_fwd (unnormalised): lane t, x[k2] = bin t + 8 k2 in,
 // samples t + 8q out in x[q].
-__device__ __forceinline__ void fft64_inv(float2 (&x)[8], float2 *wr, const float2 *rd, const float2 (&w)[8])
+__device__ __forceinline__ void fft64_inv(float2 (&x)[8], float2 *wr, const float2 *rd, const float2 *w)
 {
     dft8p<true>(x);
 #pragma unroll
@@ -167,7 +167,10 @@ __device__ __forceinline__ void fft64_inv(float2 (&x)[8], float2 *wr, const floa
     for (int k = 0; k < 8; ++k) x[k] = rd[k];
     __syncwarp();
 #pragma unroll
-    for (int k = 1; k < 8; ++k) x[k] = c_mul(x[k], make_float2(w[k].x, -w[k].y));
+    for (int k = 1; k < 8; ++k) {
+        const float2 wk = w[k];
+        x[k] = c_mul(x[k], make_float2(wk.x, -wk.y));
+    }
     dft8p<true>(x);
 }
 
@@ -306,6 +309,7 @@ __global__ void __launch_bounds__(OS_NT, MINB)
     extern __shared__ __align__(16) float osm[];
     __shared__ __align__(16) OsJob sj[3];
     __shared__ __align__(16) OsTileInfo st[3];
+    __shared__ float2 tws[8 * 9];  // twiddles w64^(t k), row t padded to 9 (conflict-free rows)
 
     const int grid = gridDim.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -319,6 +323,7 @@ __global__ void __launch_bounds__(OS_NT, MINB)
         float *dst = reinterpret_cast<float *>(&sj[slot]);
         for (int i = lane; i < (int)(sizeof(OsJob) / 16); i += 32) cp_async16(dst + 4 * i, src + 4 * i, 16);
     };
+    if (threadIdx.x < 64) tws[(threadIdx.x >> 3) * 9 + (threadIdx.x & 7)] = c_tw64[(threadIdx.x >> 3) * (threadIdx.x & 7)];
     if (warp == 0) {
         fetch(0, tiles[tile]);
         if (tile + grid < ntiles) fetch(1, tiles[tile + grid]);
@@ -335,9 +340,7 @@ __global__ void __launch_bounds__(OS_NT, MINB)
     float2 *const gs = reinterpret_cast<float2 *>(osm + 2 * stage_floats) + g * OS_SCR;
     float2 *const wr = gs + t;
     const float2 *const rd = gs + 9 * t;
-    float2 w[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) w[k] = c_tw64[(t * k) & 63];
+    const float2 *const w = tws + 9 * t;  // w[k] = w64^(t k)
 
     // first step: chunk 0 of the first tile
     {
@@ -393,43 +396,15 @@ __global__ void __launch_bounds__(OS_NT, MINB)
         const bool same = ch + 1 < J.nchunks;
         const bool has_next = same || tile + grid < ntiles;
 
-        // ---- request the next step's input ---------------------------------
-        if (same) {
-            // this tile's next chunk, slots [hs, ..): positions >= c0 + C,
-            // which this step does not store
-            const int hs = J.hs;
-            os_stage<XP>(nxt, J, base, nreal, p0 + C - J.delta, hs, os_slots(J, min(OS_M, J.nblocks - (ch + 1) * OS_M), XP),
-                         (T.flags >> 8) & 1);
-            cp_async_commit();
-            // slots [0, hs): inputs this step overwrites, carried in shared memory
-            if (XP) {
-                const int row = threadIdx.x >> 3, c = threadIdx.x & 7;  // hs <= 16: 4 float4 per row
-                if (4 * c < hs)
-                    reinterpret_cast<float4 *>(nxt + row * J.RS)[c] =
-                        reinterpret_cast<const float4 *>(in + row * J.RS + C)[c];
-            } else {
-                const float4 *hsrc = reinterpret_cast<const float4 *>(in + C * OS_RS);
-                float4 *hdst = reinterpret_cast<float4 *>(nxt);
-                for (int i = threadIdx.x; i < hs * (OS_RS / 4); i += OS_NT) hdst[i] = hsrc[i];
-            }
-        } else if (has_next) {
-            // first chunk of the next tile (other lines: no overlap with this step's stores)
-            const OsJob &Jn = sj[slot1];
-            const OsTileInfo Tn = st[slot1];
-            os_stage<XP>(nxt, Jn, os_tile_base(Jn, Tn), Tn.flags & 63, Jn.ofirst - Jn.r - Jn.delta, 0,
-                         os_slots(Jn, min(OS_M, Jn.nblocks), XP), (Tn.flags >> 8) & 1);
-            cp_async_commit();
-        }
-
-        // ---- one block of one pair per group: FFT-64, multiply, inverse,
-        // outputs straight to global memory -------------------------------
+        // ---- this step's samples into registers first (their shared-memory
+        // latency overlaps the requests below) ----------------------------
         const int seg0 = blk * L;
+        const int64_t ls = J.line_stride, ps = J.pos_stride;
+        const float b = J.b;
+        const bool va = 2 * pair < nreal, vb = 2 * pair + 1 < nreal;  // real lines of this pair
+        const unsigned qmask = J.qmask[t];  // samples t + 8q that are outputs of the block
+        float2 x[8];
         if (blk < nb) {
-            const int64_t ls = J.line_stride, ps = J.pos_stride;
-            const float b = J.b;
-            const bool va = 2 * pair < nreal, vb = 2 * pair + 1 < nreal;  // real lines of this pair
-            const unsigned qmask = J.qmask[t];  // samples t + 8q that are outputs of the block
-            float2 x[8];
             if (XP) {
                 const float *ra = in + (2 * pair) * J.RS + J.delta + seg0 + t;
                 const float *rb = ra + J.RS;
@@ -465,6 +440,39 @@ __global__ void __launch_bounds__(OS_NT, MINB)
 #pragma unroll
                 for (int q = 0; q < 8; ++q) x[q] = sp[q * 8 * (OS_RS / 2)];
             }
+        }
+
+        // ---- request the next step's input ---------------------------------
+        if (same) {
+            // this tile's next chunk, slots [hs, ..): positions >= c0 + C,
+            // which this step does not store
+            const int hs = J.hs;
+            os_stage<XP>(nxt, J, base, nreal, p0 + C - J.delta, hs, os_slots(J, min(OS_M, J.nblocks - (ch + 1) * OS_M), XP),
+                         (T.flags >> 8) & 1);
+            cp_async_commit();
+            // slots [0, hs): inputs this step overwrites, carried in shared memory
+            if (XP) {
+                const int row = threadIdx.x >> 3, c = threadIdx.x & 7;  // hs <= 16: 4 float4 per row
+                if (4 * c < hs)
+                    reinterpret_cast<float4 *>(nxt + row * J.RS)[c] =
+                        reinterpret_cast<const float4 *>(in + row * J.RS + C)[c];
+            } else {
+                const float4 *hsrc = reinterpret_cast<const float4 *>(in + C * OS_RS);
+                float4 *hdst = reinterpret_cast<float4 *>(nxt);
+                for (int i = threadIdx.x; i < hs * (OS_RS / 4); i += OS_NT) hdst[i] = hsrc[i];
+            }
+        } else if (has_next) {
+            // first chunk of the next tile (other lines: no overlap with this step's stores)
+            const OsJob &Jn = sj[slot1];
+            const OsTileInfo Tn = st[slot1];
+            os_stage<XP>(nxt, Jn, os_tile_base(Jn, Tn), Tn.flags & 63, Jn.ofirst - Jn.r - Jn.delta, 0,
+                         os_slots(Jn, min(OS_M, Jn.nblocks), XP), (Tn.flags >> 8) & 1);
+            cp_async_commit();
+        }
+
+        // ---- one block of one pair per group: FFT-64, multiply, inverse,
+        // outputs straight to global memory -------------------------------
+        if (blk < nb) {
             fft64_fwd(x, wr, rd, w);
 #pragma unroll
             for (int q = 0; q < 8; ++q) x[q] = p_mul(x[q], J.HH[t + 8 * q]);
