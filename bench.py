@@ -33,7 +33,7 @@ METRIC = "voxel-steps/s"
 # ncu dram__bytes_read.sum + dram__bytes_write.sum per axis-pass launch of this
 # workload (8 fields of 512x256x384), scaled by voxels from the 512x256x128
 # capture in profiles/os_pass_pipe_512x256x128.md (3 x 1021 MB).
-AXIS_TRAFFIC_BYTES = 3.063e9
+AXIS_TRAFFIC_BYTES = 3.059e9
 
 
 def peaks():
