@@ -345,7 +345,8 @@ def run_cfg3(args):
                                   "because the offered load exceeds the device's capacity"},
             "requests": {k: st[k] for k in ("submitted", "admitted", "completed", "rejected", "queued", "active",
                                             "rounds")},
-            "hbm_peak_bytes": st["hbm_peak"], "busy_s": st["busy_s"]}
+            "hbm_peak_bytes": st["hbm_peak"], "busy_s": st["busy_s"], "device_s": st["device_s"],
+            "rounds_per_s": st["rounds"] / max(elapsed, 1e-9)}
     print(json.dumps(line), flush=True)
 
 

@@ -182,9 +182,11 @@ vfd_status vfd_diffuse_host(vfd_world *w, const float *const *host_in,
 /* ---- batched ensembles (sensitivity-analysis ensembles of many worlds) --
  * A batch references (does not own) n_worlds worlds on one device; they
  * must outlive it.  vfd_batch_tick is vfd_tick on every world, but every
- * field of every world goes through one kernel launch per axis pass per
- * substep, and the whole tick is captured once into a CUDA graph and
- * replayed (re-captured when n_substeps or a world's sources change).
+ * field of every world goes through one persistent kernel launch per axis
+ * pass per substep.  Once the same n_substeps and source lists have run two
+ * ticks in a row the tick is captured into a CUDA graph and replayed
+ * (re-captured when n_substeps or a world's sources change); a batch used
+ * for a single tick launches directly.
  * The reference runs worlds one at a time and its chemicals one at a time
  * (Diffuser.cpp:300-341); it has no batched form. */
 typedef struct vfd_batch vfd_batch;
@@ -236,6 +238,7 @@ typedef struct vfd_server_stats {
     double voxel_steps_done;
     double p50_latency_s, p99_latency_s, mean_latency_s;  /* submit -> done   */
     size_t hbm_in_use, hbm_peak;
+    double device_s;                    /* device time of the rounds (CUDA events) */
 } vfd_server_stats;
 
 vfd_status vfd_server_create(int device, size_t hbm_budget_bytes, int max_active, int substeps_per_tick,

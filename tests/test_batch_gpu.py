@@ -67,13 +67,18 @@ def test_batch_recaptures_when_sources_change(gpu):
     w1, _ = make_world((40, 30, 20), [1.0, 1.0, 1.0], [0.0, 0.0, 0.0], 1, 0, n_src=0, nf=1)
     w2, _ = make_world((40, 30, 20), [1.0, 1.0, 1.0], [0.0, 0.0, 0.0], 1, 0, n_src=0, nf=1)
     before = [w1.download(0).astype(np.float64).sum()]
+    # direct, captured, replayed; sources change; direct, captured, replayed
     with vfd.Batch([w1]) as b:
-        b.tick(1)
+        for _ in range(3):
+            b.tick(1)
         w1.set_sources(0, np.array([7], np.int32), np.array([2.0], np.float32))
-        b.tick(1)
-    w2.tick(1)
+        for _ in range(3):
+            b.tick(1)
+    for _ in range(3):
+        w2.tick(1)
     w2.set_sources(0, np.array([7], np.int32), np.array([2.0], np.float32))
-    w2.tick(1)
+    for _ in range(3):
+        w2.tick(1)
     np.testing.assert_allclose(w1.download(0), w2.download(0), rtol=1e-5, atol=1e-9)
     assert w1.mass()[0]["sources"] == pytest.approx(2.0)
     del before

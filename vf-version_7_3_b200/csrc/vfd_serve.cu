@@ -9,9 +9,11 @@
 //   * a round advances every active request by one tick: all their fields go
 //     through one launch per axis pass per substep (vfd_batch, replayed as a
 //     CUDA graph while the active set is unchanged);
-//   * a request that finished its ticks is retired (totals, optional
-//     download) and its memory and slot are freed before the next round's
-//     admission, so new arrivals join while others are still on the device.
+//   * while a round runs, the requests finishing with it are known: new
+//     arrivals are admitted into their slots and the next round's batch is
+//     built on the host; after the round the finished requests are retired
+//     (totals, optional download) and their memory is freed, so new arrivals
+//     join while others are still on the device.
 // The reference has no serving layer: it diffuses one world per tick from
 // WHWorld::go (woundHealingWorld.cpp:2013-2026).
 #include <cuda_runtime.h>
@@ -77,10 +79,12 @@ struct vfd_server {
 
     // scheduler-owned
     std::vector<std::shared_ptr<Request>> active;
+    std::vector<std::pair<vfd_world *, size_t>> dead;  // retired worlds not yet destroyed
     vfd_batch *batch = nullptr;
     bool set_changed = true;
     size_t in_use = 0;
     cudaStream_t stream = nullptr;
+    cudaEvent_t ev_round[2] = {nullptr, nullptr};  // brackets each round on `stream`
     std::thread worker;
     std::string err;
 
@@ -163,6 +167,9 @@ int admit(vfd_server *s, const std::shared_ptr<Request> &r, std::string &msg)
     return VFD_OK;
 }
 
+// Reads a finished request's results; its world is destroyed later (`dead`),
+// after the next round has been launched, because freeing device memory
+// waits for the device.
 int retire(vfd_server *s, const std::shared_ptr<Request> &r, std::string &msg)
 {
     int st = VFD_OK;
@@ -170,58 +177,94 @@ int retire(vfd_server *s, const std::shared_ptr<Request> &r, std::string &msg)
     for (int f = 0; f < r->nf && st == VFD_OK && !r->result.empty(); ++f)
         if (r->result[f]) st = vfd_download_field(r->world, f, r->result[f], s->stream);
     if (st != VFD_OK) msg = vfd_last_error(r->world);
-    vfd_world_destroy(r->world);
+    s->dead.push_back({r->world, r->bytes});
     r->world = nullptr;
     return st;
 }
 
+// Destroys the worlds of retired requests and returns their memory to the budget.
+void bury(vfd_server *s)
+{
+    if (s->dead.empty()) return;
+    for (auto &d : s->dead) {
+        vfd_world_destroy(d.first);
+        s->in_use -= d.second;
+    }
+    s->dead.clear();
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->st.hbm_in_use = s->in_use;
+}
+
+// Takes requests off the queue while slots and budget allow (FIFO; a request
+// larger than the whole budget is rejected).  `occupied`: slots in use.
+std::vector<std::shared_ptr<Request>> select_admissions(vfd_server *s, int occupied, size_t used)
+{
+    std::vector<std::shared_ptr<Request>> out;
+    std::unique_lock<std::mutex> lk(s->mu);
+    int slots = s->max_active - occupied;
+    while (!s->pending.empty() && slots > 0) {
+        auto r = s->pending.front();
+        const size_t est = estimate_bytes(*r);
+        if (est > s->budget) {
+            s->pending.pop_front();
+            s->st.queued = (int64_t)s->pending.size();
+            lk.unlock();
+            finish(s, r, VFD_ERR_BUDGET, "request larger than the HBM budget");
+            lk.lock();
+            continue;
+        }
+        if (used + est > s->budget) break;  // FIFO: wait for memory
+        used += est;
+        out.push_back(r);
+        s->pending.pop_front();
+        --slots;
+    }
+    s->st.queued = (int64_t)s->pending.size();
+    return out;
+}
+
+// Creates the worlds of selected requests; returns those that are resident.
+std::vector<std::shared_ptr<Request>> admit_all(vfd_server *s, const std::vector<std::shared_ptr<Request>> &sel)
+{
+    std::vector<std::shared_ptr<Request>> ok;
+    for (auto &r : sel) {
+        std::string msg;
+        r->info.t_admit = s->now();
+        const int st = admit(s, r, msg);
+        if (st != VFD_OK) {
+            finish(s, r, st, msg);
+            continue;
+        }
+        s->in_use += r->bytes;
+        ok.push_back(r);
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->st.admitted++;
+    }
+    return ok;
+}
+
+// The scheduler overlaps host work with the device: while a round runs, the
+// requests that finish with it are already known, so new requests are
+// admitted and the next round's batch is built before the round ends; after
+// it ends the finished requests are retired and the next round starts at once.
 void scheduler(vfd_server *s)
 {
     cudaSetDevice(s->device);
     for (;;) {
-        // ---- admission ----------------------------------------------------
-        std::vector<std::shared_ptr<Request>> admit_now;
+        // ---- admission while the device is idle ----------------------------
+        if (s->active.empty()) bury(s);
         {
             std::unique_lock<std::mutex> lk(s->mu);
             s->cv_work.wait(lk, [&] { return s->stop || !s->pending.empty() || !s->active.empty(); });
             if (s->stop) break;
-            size_t used = s->in_use;
-            int slots = s->max_active - (int)s->active.size();
-            while (!s->pending.empty() && slots > 0) {
-                auto &r = s->pending.front();
-                const size_t est = estimate_bytes(*r);
-                if (est > s->budget) {
-                    auto bad = r;
-                    s->pending.pop_front();
-                    s->st.queued = (int64_t)s->pending.size();
-                    lk.unlock();
-                    finish(s, bad, VFD_ERR_BUDGET, "request larger than the HBM budget");
-                    lk.lock();
-                    continue;
-                }
-                if (used + est > s->budget) break;  // FIFO: wait for memory
-                used += est;
-                admit_now.push_back(r);
-                s->pending.pop_front();
-                --slots;
-            }
-            s->st.queued = (int64_t)s->pending.size();
         }
-        for (auto &r : admit_now) {
-            std::string msg;
-            r->info.t_admit = s->now();
-            const int st = admit(s, r, msg);
-            if (st != VFD_OK) {
-                finish(s, r, st, msg);
-                continue;
-            }
-            s->in_use += r->bytes;
-            s->active.push_back(r);
-            s->set_changed = true;
-            std::lock_guard<std::mutex> lk(s->mu);
-            s->st.admitted++;
+        {
+            auto got = admit_all(s, select_admissions(s, (int)s->active.size(), s->in_use));
+            if (!got.empty()) s->set_changed = true;
+            s->active.insert(s->active.end(), got.begin(), got.end());
         }
         if (s->active.empty()) {
+            bury(s);
             std::lock_guard<std::mutex> lk(s->mu);
             if (s->busy_since >= 0) {
                 s->st.busy_s += s->now() - s->busy_since;
@@ -233,8 +276,7 @@ void scheduler(vfd_server *s)
             std::lock_guard<std::mutex> lk(s->mu);
             if (s->busy_since < 0) s->busy_since = s->now();
         }
-        // ---- one round: every active request advances one tick -----------
-        if (s->set_changed) {
+        if (s->set_changed || !s->batch) {
             if (s->batch) vfd_batch_destroy(s->batch);
             s->batch = nullptr;
             std::vector<vfd_world *> ws;
@@ -244,41 +286,76 @@ void scheduler(vfd_server *s)
                 for (auto &r : s->active) {
                     vfd_world_destroy(r->world);
                     r->world = nullptr;
+                    s->in_use -= r->bytes;
                     finish(s, r, VFD_ERR_CUDA, msg);
                 }
                 s->active.clear();
-                s->in_use = 0;
                 continue;
             }
             s->set_changed = false;
         }
+
+        // ---- one round: every active request advances one tick -----------
+        cudaEventRecord(s->ev_round[0], s->stream);
         vfd_status st = vfd_batch_tick(s->batch, s->substeps, s->stream);
+        cudaEventRecord(s->ev_round[1], s->stream);
+
+        // while it runs: admit into the slots of requests finishing now and
+        // build the next round's batch
+        std::vector<std::shared_ptr<Request>> survivors, joining;
+        vfd_batch *next = nullptr;
+        bool next_changed = false;
+        if (st == VFD_OK) {
+            for (auto &r : s->active)
+                if (r->ticks_done + 1 < r->ticks) survivors.push_back(r);
+            joining = admit_all(s, select_admissions(s, (int)survivors.size(), s->in_use));
+            next_changed = survivors.size() != s->active.size() || !joining.empty();
+            if (next_changed && survivors.size() + joining.size() > 0) {
+                std::vector<vfd_world *> ws;
+                for (auto &r : survivors) ws.push_back(r->world);
+                for (auto &r : joining) ws.push_back(r->world);
+                if (vfd_batch_create(ws.data(), (int)ws.size(), &next) != VFD_OK) next = nullptr;  // rebuilt later
+            }
+        }
+        bury(s);  // last round's retired worlds (waits for the device)
         if (st == VFD_OK && cudaStreamSynchronize(s->stream) != cudaSuccess) st = VFD_ERR_CUDA;
+        float round_ms = 0.0f;
+        if (st == VFD_OK) cudaEventElapsedTime(&round_ms, s->ev_round[0], s->ev_round[1]);
         {
             std::lock_guard<std::mutex> lk(s->mu);
             s->st.rounds++;
+            s->st.device_s += 1e-3 * round_ms;
         }
-        std::vector<std::shared_ptr<Request>> still;
-        for (auto &r : s->active) {
-            if (st != VFD_OK) {
+        if (st != VFD_OK) {
+            const std::string msg = vfd_batch_last_error(s->batch);
+            for (auto &r : s->active) {
                 vfd_world_destroy(r->world);
                 r->world = nullptr;
                 s->in_use -= r->bytes;
-                finish(s, r, st, vfd_batch_last_error(s->batch));
-                continue;
+                finish(s, r, st, msg);
             }
-            r->ticks_done++;
-            if (r->ticks_done >= r->ticks) {
-                std::string msg;
-                const int rs = retire(s, r, msg);
-                s->in_use -= r->bytes;
-                finish(s, r, rs, msg);
-            } else {
-                still.push_back(r);
+            if (next) vfd_batch_destroy(next);
+            vfd_batch_destroy(s->batch);
+            s->batch = nullptr;
+            s->active = joining;  // admitted during the failed round: not part of it
+            s->set_changed = true;
+        } else {
+            for (auto &r : s->active) {
+                r->ticks_done++;
+                if (r->ticks_done >= r->ticks) {
+                    std::string msg;
+                    const int rs = retire(s, r, msg);
+                    finish(s, r, rs, msg);
+                }
+            }
+            if (next_changed) {
+                vfd_batch_destroy(s->batch);
+                s->batch = next;
+                s->set_changed = next == nullptr;
+                survivors.insert(survivors.end(), joining.begin(), joining.end());
+                s->active.swap(survivors);
             }
         }
-        if (still.size() != s->active.size()) s->set_changed = true;
-        s->active.swap(still);
         std::lock_guard<std::mutex> lk(s->mu);
         s->st.active = (int64_t)s->active.size();
         s->st.hbm_in_use = s->in_use;
@@ -287,6 +364,7 @@ void scheduler(vfd_server *s)
     // shutdown: drop what is still resident
     if (s->batch) vfd_batch_destroy(s->batch);
     s->batch = nullptr;
+    bury(s);
     for (auto &r : s->active) {
         vfd_world_destroy(r->world);
         r->world = nullptr;
@@ -316,11 +394,17 @@ vfd_status vfd_server_create(int device, size_t hbm_budget_bytes, int max_active
     cudaGetDevice(&prev);
     cudaSetDevice(device);
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-    cudaSetDevice(prev);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_round[0]);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_round[1]);
     if (e != cudaSuccess) {
+        for (auto &ev : s->ev_round)
+            if (ev) cudaEventDestroy(ev);
+        if (s->stream) cudaStreamDestroy(s->stream);
+        cudaSetDevice(prev);
         delete s;
         return VFD_ERR_CUDA;
     }
+    cudaSetDevice(prev);
     s->worker = std::thread(scheduler, s);
     *out = s;
     return VFD_OK;
@@ -434,6 +518,7 @@ vfd_status vfd_server_destroy(vfd_server *s)
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(s->device);
+    for (auto &ev : s->ev_round) cudaEventDestroy(ev);
     cudaStreamDestroy(s->stream);
     cudaSetDevice(prev);
     delete s;

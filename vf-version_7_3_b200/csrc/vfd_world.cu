@@ -670,7 +670,9 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
     w->src_amt.resize(w->nf);
     w->src_begin.assign(w->nf, 0);
     w->src_count.assign(w->nf, 0);
-    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(e, "cudaDeviceSynchronize");
+    // the set-up above ran on the legacy stream; work on other streams (a
+    // batch running on this device) is not waited for
+    if ((e = cudaStreamSynchronize(0)) != cudaSuccess) return bail(e, "cudaStreamSynchronize");
     cudaSetDevice(prev);
     *out = w;
     return VFD_OK;
@@ -1275,6 +1277,7 @@ struct vfd_batch {
     cudaGraphExec_t exec = nullptr;
     int graph_substeps = -1;
     uint64_t graph_launches = 0;
+    int same_ticks = 0;  // ticks in a row with the current substep count and sources
     std::vector<uint64_t> gens;
     std::string err;
 };
@@ -1441,38 +1444,51 @@ vfd_status vfd_batch_tick(vfd_batch *b, int n_substeps, void *stream)
     if (!b) return VFD_ERR_INVALID_ARG;
     if (n_substeps < 1) return bfail(b, VFD_ERR_INVALID_ARG, "n_substeps must be >= 1");
     DeviceGuard g(b->device);
-    bool stale = (b->exec == nullptr) || (b->graph_substeps != n_substeps);
+    // The tick is captured into a CUDA graph once the same configuration
+    // (substep count, source lists) has run twice in a row; a batch that
+    // lives for a single tick (a server round whose active set changes)
+    // launches its kernels directly and pays no capture.
+    bool stale = b->graph_substeps != n_substeps;
     for (size_t i = 0; i < b->worlds.size(); ++i) {
         vfd_status st = sync_sources(b->worlds[i]);
         if (st != VFD_OK) return bfail(b, st, b->worlds[i]->err);
         if (b->gens[i] != b->worlds[i]->src_gen) stale = true;
     }
-    VFD_BCUDA(b, cudaEventRecord(b->ev_in, (cudaStream_t)stream));
-    VFD_BCUDA(b, cudaStreamWaitEvent(b->st, b->ev_in, 0));
     if (stale) {
         if (b->exec) cudaGraphExecDestroy(b->exec);
         if (b->graph) cudaGraphDestroy(b->graph);
         b->exec = nullptr;
         b->graph = nullptr;
-        const uint64_t before = g_launches.load();
-        VFD_BCUDA(b, cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
-        vfd_status st = batch_enqueue(b, n_substeps);
-        cudaGraph_t graph = nullptr;
-        cudaError_t ce = cudaStreamEndCapture(b->st, &graph);
-        if (st != VFD_OK) {
-            if (graph) cudaGraphDestroy(graph);
-            return st;
-        }
-        if (ce != cudaSuccess) return bfail(b, VFD_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
-        b->graph = graph;
-        b->graph_launches = g_launches.load() - before;
-        g_launches.fetch_sub(b->graph_launches);  // captured, not executed
-        VFD_BCUDA(b, cudaGraphInstantiate(&b->exec, b->graph, 0));
         b->graph_substeps = n_substeps;
         for (size_t i = 0; i < b->worlds.size(); ++i) b->gens[i] = b->worlds[i]->src_gen;
+        b->same_ticks = 0;
     }
-    VFD_BCUDA(b, cudaGraphLaunch(b->exec, b->st));
-    g_launches.fetch_add(b->graph_launches);
+    ++b->same_ticks;
+    VFD_BCUDA(b, cudaEventRecord(b->ev_in, (cudaStream_t)stream));
+    VFD_BCUDA(b, cudaStreamWaitEvent(b->st, b->ev_in, 0));
+    if (!b->exec && b->same_ticks < 2) {
+        vfd_status st = batch_enqueue(b, n_substeps);
+        if (st != VFD_OK) return st;
+    } else {
+        if (!b->exec) {
+            const uint64_t before = g_launches.load();
+            VFD_BCUDA(b, cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+            vfd_status st = batch_enqueue(b, n_substeps);
+            cudaGraph_t graph = nullptr;
+            cudaError_t ce = cudaStreamEndCapture(b->st, &graph);
+            if (st != VFD_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return st;
+            }
+            if (ce != cudaSuccess) return bfail(b, VFD_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
+            b->graph = graph;
+            b->graph_launches = g_launches.load() - before;
+            g_launches.fetch_sub(b->graph_launches);  // captured, not executed
+            VFD_BCUDA(b, cudaGraphInstantiate(&b->exec, b->graph, 0));
+        }
+        VFD_BCUDA(b, cudaGraphLaunch(b->exec, b->st));
+        g_launches.fetch_add(b->graph_launches);
+    }
     VFD_BCUDA(b, cudaEventRecord(b->ev_out, b->st));
     VFD_BCUDA(b, cudaStreamWaitEvent((cudaStream_t)stream, b->ev_out, 0));
     return VFD_OK;

@@ -96,7 +96,8 @@ class ServerStats(C.Structure):
                 ("rejected", C.c_int64), ("active", C.c_int64), ("queued", C.c_int64),
                 ("rounds", C.c_int64), ("busy_s", C.c_double), ("voxel_steps_done", C.c_double),
                 ("p50_latency_s", C.c_double), ("p99_latency_s", C.c_double),
-                ("mean_latency_s", C.c_double), ("hbm_in_use", C.c_size_t), ("hbm_peak", C.c_size_t)]
+                ("mean_latency_s", C.c_double), ("hbm_in_use", C.c_size_t), ("hbm_peak", C.c_size_t),
+                ("device_s", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
