@@ -1,0 +1,27 @@
+// vfd_rf.h -- axis pass with the FFT-64 of each block held by one thread
+// (vfd_rf.cu).  Jobs are overlap-save jobs (vfd_os.h) of radius <= RF_RMAX;
+// tiles are 64 lines.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "vfd_os.h"
+
+namespace vfd {
+
+constexpr int RF_RMAX = 8;    // largest radius of the register-FFT pass
+constexpr int RF_LINES = 64;  // lines per tile (32 line pairs, one warp)
+
+// Whether job j (its other fields set) can use the register-FFT pass.
+bool rf_eligible(const OsJob &j);
+// Appends the 64-line tiles of job `job` to `out` (flags: bits 0-7 real
+// lines, bit 8: pair loads of 8 bytes apply).
+void rf_append_tiles(const OsJob &j, int job, std::vector<OsTileInfo> &out);
+// Uploads the FFT-64 twiddles to the current device (outside stream capture).
+cudaError_t rf_prepare();
+// One launch over `ntiles` tiles of jobs (any radius <= RF_RMAX) that all
+// belong to `axis`; pairs8: every tile allows 8-byte pair accesses (flag bit 8).
+cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int axis, bool pairs8, cudaStream_t st);
+
+}  // namespace vfd

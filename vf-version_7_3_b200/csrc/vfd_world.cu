@@ -22,6 +22,7 @@
 #include "vfd_general.h"
 #include "vfd_internal.h"
 #include "vfd_os.h"
+#include "vfd_rf.h"
 
 namespace vfd {
 
@@ -188,6 +189,61 @@ static void twiddles(int F, std::vector<float2> &out)
 
 using namespace vfd;
 
+// A register-FFT launch of one axis (tiles of every radius).
+struct RfGroup {
+    int r = 0;  // unused: the kernel reads each tile's radius from its job
+    bool pairs8 = false;   // every tile allows 8-byte pair accesses
+    int ntiles = 0;
+    OsTileInfo *d_tiles = nullptr;
+};
+
+static bool rf_enabled()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("VFD_RF");
+        on = (e && e[0] == '0') ? 0 : 1;
+    }
+    return on == 1;
+}
+
+// Tiles of jobs[0..n) (all rf-eligible) for one launch, uploaded.  Job
+// indices in the tiles are positions in `jobs`.
+static cudaError_t build_rf_groups(const OsJob *jobs, int n, std::vector<RfGroup> &out)
+{
+    std::vector<OsTileInfo> t;
+    for (int i = 0; i < n; ++i) rf_append_tiles(jobs[i], i, t);
+    if (t.empty()) return cudaSuccess;
+    RfGroup g;
+    g.r = 0;
+    g.ntiles = (int)t.size();
+    g.pairs8 = true;
+    for (const auto &ti : t) g.pairs8 = g.pairs8 && ((ti.flags >> 8) & 1);
+    cudaError_t e = cudaMalloc(&g.d_tiles, sizeof(OsTileInfo) * t.size());
+    if (e == cudaSuccess) e = cudaMemcpy(g.d_tiles, t.data(), sizeof(OsTileInfo) * t.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(g.d_tiles);
+        return e;
+    }
+    out.push_back(g);
+    return cudaSuccess;
+}
+
+static void free_rf_groups(std::vector<RfGroup> &g)
+{
+    for (auto &x : g) cudaFree(x.d_tiles);
+    g.clear();
+}
+
+static cudaError_t launch_rf_groups(const OsJob *jobs, const std::vector<RfGroup> &g, int axis, cudaStream_t st)
+{
+    for (const auto &x : g) {
+        cudaError_t e = launch_rf(jobs, x.d_tiles, x.ntiles, axis, x.pairs8, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 struct vfd_world {
     int device = 0;
     int nx = 0, ny = 0, nz = 0, nf = 0;
@@ -205,6 +261,9 @@ struct vfd_world {
     std::vector<int> os_tiles[3];          // per field
     OsTileInfo *d_os_tiles[3] = {nullptr, nullptr, nullptr};    // all-field launches
     OsTileInfo *d_os_ftiles[3] = {nullptr, nullptr, nullptr};   // single-field launches, [field][tiles]
+    bool use_rf[3] = {false, false, false};       // register-FFT pass (radius <= RF_RMAX)
+    std::vector<RfGroup> rf[3];                   // all-field launches
+    std::vector<std::vector<RfGroup>> rf_field[3];  // single-field launches
 
     float *d_fields = nullptr;
     float2 *d_tw[3] = {nullptr, nullptr, nullptr};
@@ -282,6 +341,9 @@ static void release(vfd_world *w)
     for (int a = 0; a < 3; ++a) {
         cudaFree(w->d_os_tiles[a]);
         cudaFree(w->d_os_ftiles[a]);
+        free_rf_groups(w->rf[a]);
+        for (auto &g : w->rf_field[a]) free_rf_groups(g);
+        w->rf_field[a].clear();
     }
     cudaFree(w->d_err);
     cudaFree(w->d_src_idx);
@@ -637,6 +699,18 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
             if ((e = upload_vec(&w->d_os_tiles[a], all)) != cudaSuccess ||
                 (e = upload_vec(&w->d_os_ftiles[a], one)) != cudaSuccess)
                 return bail(e, "os tiles");
+        }
+        for (int a = 0; a < 3 && rf_enabled(); ++a) {
+            bool ok = w->use_os[a];
+            for (int f = 0; f < w->nf; ++f) ok = ok && rf_eligible(oj[(size_t)a * w->nf + f]);
+            if (!ok) continue;
+            if ((e = rf_prepare()) != cudaSuccess) return bail(e, "register-FFT twiddles");
+            if ((e = build_rf_groups(&oj[(size_t)a * w->nf], w->nf, w->rf[a])) != cudaSuccess) return bail(e, "rf tiles");
+            w->rf_field[a].resize(w->nf);
+            for (int f = 0; f < w->nf; ++f)
+                if ((e = build_rf_groups(&oj[(size_t)(3 + a) * w->nf + f], 1, w->rf_field[a][f])) != cudaSuccess)
+                    return bail(e, "rf tiles");
+            w->use_rf[a] = true;
         }
     }
     if ((e = cudaMalloc(&w->d_dep, sizeof(DepositJob) * 2 * w->nf)) != cudaSuccess) return bail(e, "cudaMalloc deposit jobs");
@@ -1088,7 +1162,13 @@ static vfd_status enqueue_tick(vfd_world *w, int field, int n_substeps, cudaStre
             VFD_CUDA(w, cudaMemsetAsync(w->d_mass + (int64_t)field * MS_COUNT, 0, sizeof(double) * MS_COUNT, st));
         for (int a = 0; a < 3; ++a) {
             LaunchTimer lt(w, a, st);
-            if (w->use_os[a]) {
+            if (w->use_rf[a]) {
+                if (field < 0)
+                    VFD_CUDA(w, launch_rf_groups(w->d_osjobs + a * w->nf, w->rf[a], a, st));
+                else
+                    VFD_CUDA(w, launch_rf_groups(w->d_osjobs + 3 * w->nf + a * w->nf + field, w->rf_field[a][field],
+                                                 a, st));
+            } else if (w->use_os[a]) {
                 const OsJob *jobs =
                     field < 0 ? w->d_osjobs + a * w->nf : w->d_osjobs + 3 * w->nf + a * w->nf + field;
                 int tiles = 0;
@@ -1271,6 +1351,8 @@ struct vfd_batch {
     OsJob *d_osjobs = nullptr;  // [3][njobs]
     int os_tiles[3] = {0, 0, 0};
     OsTileInfo *d_os_tiles[3] = {nullptr, nullptr, nullptr};
+    bool use_rf[3] = {false, false, false};
+    std::vector<RfGroup> rf[3];
     cudaStream_t st = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     cudaGraph_t graph = nullptr;
@@ -1307,7 +1389,10 @@ static void batch_release(vfd_batch *b)
     if (b->graph) cudaGraphDestroy(b->graph);
     cudaFree(b->d_jobs);
     cudaFree(b->d_osjobs);
-    for (int a = 0; a < 3; ++a) cudaFree(b->d_os_tiles[a]);
+    for (int a = 0; a < 3; ++a) {
+        cudaFree(b->d_os_tiles[a]);
+        free_rf_groups(b->rf[a]);
+    }
     if (b->ev_in) cudaEventDestroy(b->ev_in);
     if (b->ev_out) cudaEventDestroy(b->ev_out);
     if (b->st) cudaStreamDestroy(b->st);
@@ -1315,6 +1400,23 @@ static void batch_release(vfd_batch *b)
 }
 
 extern "C" {
+
+// Register-FFT groups of every axis whose jobs (oj: [axis][njobs]) are all eligible.
+static cudaError_t batch_rf_setup(vfd_batch *b, const std::vector<OsJob> &oj)
+{
+    if (!rf_enabled()) return cudaSuccess;
+    for (int a = 0; a < 3; ++a) {
+        if (!b->use_os[a]) continue;
+        bool ok = true;
+        for (int i = 0; i < b->njobs; ++i) ok = ok && rf_eligible(oj[(size_t)a * b->njobs + i]);
+        if (!ok) continue;
+        cudaError_t e = rf_prepare();
+        if (e == cudaSuccess) e = build_rf_groups(&oj[(size_t)a * b->njobs], b->njobs, b->rf[a]);
+        if (e != cudaSuccess) return e;
+        b->use_rf[a] = true;
+    }
+    return cudaSuccess;
+}
 
 vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **out)
 {
@@ -1387,7 +1489,8 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
             (e2 = cudaMemcpy(b->d_osjobs, oj.data(), sizeof(OsJob) * oj.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
             (e2 = upload_vec(&b->d_os_tiles[0], tile_info[0])) != cudaSuccess ||
             (e2 = upload_vec(&b->d_os_tiles[1], tile_info[1])) != cudaSuccess ||
-            (e2 = upload_vec(&b->d_os_tiles[2], tile_info[2])) != cudaSuccess) {
+            (e2 = upload_vec(&b->d_os_tiles[2], tile_info[2])) != cudaSuccess ||
+            (e2 = batch_rf_setup(b, oj)) != cudaSuccess) {
             std::string msg = std::string("batch os jobs: ") + cudaGetErrorString(e2);
             batch_release(b);
             delete b;
@@ -1424,7 +1527,9 @@ static vfd_status batch_enqueue(vfd_batch *b, int n_substeps)
         for (auto *w : b->worlds)
             VFD_BCUDA(b, cudaMemsetAsync(w->d_mass, 0, sizeof(double) * MS_COUNT * w->nf, b->st));
         for (int a = 0; a < 3; ++a) {
-            if (b->use_os[a])
+            if (b->use_rf[a])
+                VFD_BCUDA(b, launch_rf_groups(b->d_osjobs + a * b->njobs, b->rf[a], a, b->st));
+            else if (b->use_os[a])
                 VFD_BCUDA(b, launch_os(b->d_osjobs + a * b->njobs, b->d_os_tiles[a], b->os_tiles[a], b->rmin[a], a,
                                        b->st));
             else
