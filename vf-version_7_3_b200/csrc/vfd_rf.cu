@@ -247,6 +247,116 @@ __device__ __forceinline__ void rf_col_body(const OsJob &J, const OsTileInfo &T,
     }
 }
 
+// The same walk with the radius read from the job at run time: register
+// indices stay compile-time (every slot is tested against [r, r + L)), the
+// held-back outputs are indexed in shared memory.  One code body for every
+// radius keeps the kernel small enough for the instruction cache when warps
+// of different radii share an SM.
+template <bool V2>
+__device__ __forceinline__ void rf_col_body_rt(const OsJob &J, const OsTileInfo &T, const float2 *hh,
+                                               float2 (*held)[32])
+{
+    const int R = J.r, L = 64 - 2 * R;
+    const int lane = threadIdx.x;
+    const int nreal = T.flags & 255;
+    const int line = 2 * lane;
+    const bool va = line < nreal, vb = line + 1 < nreal;
+    const int n = J.n;
+    const int64_t ps = J.pos_stride;
+    float *const base = J.data + T.outer * J.outer_stride + (int64_t)(T.l0 + line) * J.line_stride;
+    const bool zlast = J.kind == PASS_Z;
+    const float keep = J.keep, b = J.b;
+    const int nblocks = (n + 2 * R + L - 1) / L;
+    auto put = [&](int o, float2 v) {
+        float *d = base + (int64_t)o * ps;
+        if (V2) {
+            *reinterpret_cast<float2 *>(d) = v;
+        } else {
+            d[0] = v.x;
+            if (vb) d[1] = v.y;
+        }
+    };
+
+    float2 lk = make_float2(0.0f, 0.0f), cv = lk, ot = lk;
+    if (va) {
+        for (int bi = 0; bi < nblocks; ++bi) {
+            const int c = -R + bi * L;
+            const int p0 = c - R;
+            float2 x[64];
+            {
+                const float *sp = base + (int64_t)p0 * ps;
+                if (V2) {
+#pragma unroll
+                    for (int i = 0; i < 64; ++i, sp += ps)
+                        x[i] = ((unsigned)(p0 + i) < (unsigned)n) ? *reinterpret_cast<const float2 *>(sp)
+                                                                  : make_float2(0.0f, 0.0f);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 64; ++i, sp += ps) {
+                        const bool in = (unsigned)(p0 + i) < (unsigned)n;
+                        x[i] = make_float2(in ? sp[0] : 0.0f, (in && vb) ? sp[1] : 0.0f);
+                    }
+                }
+            }
+            if (bi > 0)
+                for (int i = 0; i < R; ++i)
+                    if ((unsigned)(p0 + i) < (unsigned)n) put(p0 + i, held[i][lane]);
+            r_fft64_fwd(x);
+            r_modulate(x, hh);
+            r_fft64_inv(x);
+#pragma unroll
+            for (int i = 1; i < 63; ++i) {  // kept samples: i in [R, R + L), R in 1 .. 8
+                if (i < R || i >= R + L) continue;
+                const int o = c + i - R;
+                if ((unsigned)o < (unsigned)n) {
+                    float2 v = x[i];
+                    if (zlast) {
+                        cv = r_add(cv, v);
+                        v = r_mul(r_add(v, make_float2(b, b)), make_float2(keep, keep));
+                        ot = r_add(ot, v);
+                    }
+                    if (i >= L) held[i - L][lane] = v;  // stored after the next block's loads
+                    else put(o, v);
+                } else if (o >= -R && o < n + R) {
+                    lk = r_add(lk, x[i]);
+                }
+            }
+        }
+        const int clast = -R + (nblocks - 1) * L;
+        for (int i = 0; i < R; ++i) {
+            const int o = clast + L - R + i;
+            if ((unsigned)o < (unsigned)n) put(o, held[i][lane]);
+        }
+    }
+    double *mass = J.mass;
+    const double s_lk = r_warp_sum((double)(va ? lk.x : 0.0f) + (double)(vb ? lk.y : 0.0f));
+    if (J.kind == PASS_Y) {
+        if (lane == 0 && s_lk != 0.0) atomicAdd(mass + MS_LEAK_Y, s_lk);
+    } else {
+        const double s_cv = r_warp_sum((double)(va ? cv.x : 0.0f) + (double)(vb ? cv.y : 0.0f));
+        const double s_ot = r_warp_sum((double)(va ? ot.x : 0.0f) + (double)(vb ? ot.y : 0.0f));
+        if (lane == 0) {
+            if (s_lk != 0.0) atomicAdd(mass + MS_LEAK_Z, s_lk);
+            if (s_cv != 0.0) atomicAdd(mass + MS_CONV, s_cv);
+            if (s_ot != 0.0) atomicAdd(mass + MS_OUT, s_ot);
+        }
+    }
+}
+
+template <bool V2>
+__global__ void __launch_bounds__(32, 12) rf_col_rt_kernel(const OsJob *__restrict__ jobs,
+                                                           const OsTileInfo *__restrict__ tiles)
+{
+    __shared__ __align__(16) float2 hh[64];
+    __shared__ float2 held[RF_RMAX][32];
+    const OsTileInfo T = tiles[blockIdx.x];
+    const OsJob &J = jobs[T.job];
+    hh[threadIdx.x] = J.HH[threadIdx.x];
+    hh[threadIdx.x + 32] = J.HH[threadIdx.x + 32];
+    __syncwarp();
+    rf_col_body_rt<V2>(J, T, hh, held);
+}
+
 // One launch covers tiles of every radius: the CTA's job picks the variant.
 template <bool V2>
 __global__ void __launch_bounds__(32, 12) rf_col_kernel(const OsJob *__restrict__ jobs,
@@ -501,6 +611,18 @@ static bool rf_row_enabled()
     return on == 1;
 }
 
+// VFD_RF_RT=1 selects the y/z kernel that reads the radius at run time (one
+// code body) instead of the one with a compiled variant per radius.
+static bool rf_col_runtime_radius()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("VFD_RF_RT");
+        on = (e && e[0] == '1') ? 1 : 0;
+    }
+    return on == 1;
+}
+
 static std::mutex g_rf_mu;
 static bool g_rf_done[64];
 
@@ -535,7 +657,10 @@ cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, in
     }
     if (!ready && (e = rf_prepare()) != cudaSuccess) return e;
     if (axis == PASS_X) rf_row_kernel<<<ntiles, 32, 0, st>>>(jobs, tiles);
-    else if (pairs8) rf_col_kernel<true><<<ntiles, 32, 0, st>>>(jobs, tiles);
+    else if (rf_col_runtime_radius()) {
+        if (pairs8) rf_col_rt_kernel<true><<<ntiles, 32, 0, st>>>(jobs, tiles);
+        else rf_col_rt_kernel<false><<<ntiles, 32, 0, st>>>(jobs, tiles);
+    } else if (pairs8) rf_col_kernel<true><<<ntiles, 32, 0, st>>>(jobs, tiles);
     else rf_col_kernel<false><<<ntiles, 32, 0, st>>>(jobs, tiles);
     note_launch();
     return cudaGetLastError();

@@ -214,6 +214,10 @@ static cudaError_t build_rf_groups(const OsJob *jobs, int n, std::vector<RfGroup
     std::vector<OsTileInfo> t;
     for (int i = 0; i < n; ++i) rf_append_tiles(jobs[i], i, t);
     if (t.empty()) return cudaSuccess;
+    // CTAs start in tile order: grouping tiles by radius keeps the warps
+    // resident together on one compiled variant (instruction-cache locality)
+    std::stable_sort(t.begin(), t.end(),
+                     [&](const OsTileInfo &a, const OsTileInfo &b) { return jobs[a.job].r < jobs[b.job].r; });
     RfGroup g;
     g.r = 0;
     g.ntiles = (int)t.size();
