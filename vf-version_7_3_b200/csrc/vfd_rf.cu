@@ -15,9 +15,10 @@
 //   (64 lines); at each position the warp loads and stores 256 contiguous
 //   bytes straight from and to global memory.
 //   x pass (positions contiguous): a warp owns 64 rows; each block's window
-//   is loaded row by row with coalesced loads into a shared tile that keeps
-//   the two rows of a pair side by side (one float2 per position), each
-//   thread reads its pair's column, and outputs go back the same way.
+//   is copied row by row with 16-byte cp.async into a shared tile, each
+//   thread reads its pair's two rows, and outputs go back the same way with
+//   16-byte stores (rows 16-byte aligned and n a multiple of 4; otherwise
+//   the x pass uses the overlap-save kernel).
 //
 // In place: block b's window starts r positions before its first output, so
 // it overlaps the previous block's last r outputs.  Those r outputs are held
@@ -382,26 +383,40 @@ __global__ void __launch_bounds__(32, 12) rf_col_kernel(const OsJob *__restrict_
 }
 
 // ---------------------------------------------------------------------------
-// x pass: one warp = 64 rows (32 pairs).  Shared tile of 64 rows x 65 floats;
-// row 2q of the tile is kept in tile row q and row 2q+1 in tile row 32 + q,
-// so that with the odd row length a warp's column reads (lane = pair, rows
-// lane and 32 + lane) hit 32 distinct banks.  The window is copied in with
-// 4-byte cp.async (zero-filled outside the line), so no registers hold it.
+// x pass: one warp = 64 rows (32 pairs).  Rows hold positions contiguously,
+// so blocks are moved through a shared tile with 16-byte copies:
+//   * chunks start on multiples of 4: the first output is -Rh (Rh = r
+//     rounded up to 4) and blocks keep L4 outputs (L4 = L rounded down to a
+//     multiple of 4); a block's window is the 68 positions from c - Rh, and
+//     its FFT input starts e = Rh - r positions into it;
+//   * tile rows are 68 floats; line row 2q sits in tile row q and row 2q+1
+//     in tile row 32 + q, so a warp's 16-byte column reads (lane = pair) fall
+//     on distinct bank quads (68 floats = 272 bytes = 16 mod 128);
+//   * the last Rh outputs of a block are the first Rh positions of the next
+//     window: they are held back and stored after that window has landed.
+// Needs rows 16-byte aligned and n a multiple of 4.
 // ---------------------------------------------------------------------------
-constexpr int RF_TS = 65;
+constexpr int RF_TS = 68;  // floats per tile row (17 chunks of 4)
 
-__device__ __forceinline__ void rf_cp4(float *smem, const float *gmem, bool valid)
+__device__ __forceinline__ void rf_cp16(float *smem, const float *gmem, bool valid)
 {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 4 : 0)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 16 : 0)
                  : "memory");
 }
 
+__device__ __forceinline__ int rf_trow(int row) { return (row & 1) * 32 + (row >> 1); }
+
 template <int R>
 __device__ __forceinline__ void rf_row_body(const OsJob &J, const OsTileInfo &T, const float2 *hh, float *A,
-                                            float2 (*held)[32])
+                                            float *held)
 {
     constexpr int L = 64 - 2 * R;
+    constexpr int L4 = L & ~3;          // outputs kept per block
+    constexpr int RH = (R + 3) & ~3;    // held-back outputs per block (multiple of 4)
+    constexpr int E = RH - R;           // FFT input offset in the window
+    constexpr int NST = (L4 - RH) / 4;  // chunks stored at once per row
+    constexpr int NHD = RH / 4;         // held chunks per row
     const int lane = threadIdx.x;
     const int nreal = T.flags & 255;
     const int n = J.n;
@@ -409,9 +424,6 @@ __device__ __forceinline__ void rf_row_body(const OsJob &J, const OsTileInfo &T,
     float *const base = J.data + (int64_t)T.l0 * ls;
     const float b = J.b;
     const bool masked = J.mask != 0;
-    // tile row of line row: 2q -> q, 2q + 1 -> 32 + q
-    auto trow = [](int row) { return (row & 1) * 32 + (row >> 1); };
-    // padding rule (x pass): this lane's rows inside the y/z box, box range along x
     bool in_a = 2 * lane < nreal, in_b = 2 * lane + 1 < nreal;
     const bool va = in_a, vb = in_b;
     int xlo = 0, xhi = n;
@@ -427,47 +439,59 @@ __device__ __forceinline__ void rf_row_body(const OsJob &J, const OsTileInfo &T,
             in_b = y >= J.box_lo[1] && y < J.box_hi[1] && z >= J.box_lo[2] && z < J.box_hi[2];
         }
     }
-    const int nblocks = (n + 2 * R + L - 1) / L;
+    const int nblocks = (n + R + RH + L4 - 1) / L4;
+    // stores the held-back outputs (positions pa .. pa + RH - 1) of every row
+    auto put_held = [&](int pa) {
+        for (int k = lane; k < nreal * NHD; k += 32) {
+            const int row = k / NHD, cc = k - row * NHD;
+            const int o = pa + 4 * cc;
+            if ((unsigned)o < (unsigned)n)
+                *reinterpret_cast<float4 *>(base + (int64_t)row * ls + o) =
+                    *reinterpret_cast<const float4 *>(held + row * RH + 4 * cc);
+        }
+    };
 
     double acc_in = 0.0;
     float2 lk = make_float2(0.0f, 0.0f);
     for (int bi = 0; bi < nblocks; ++bi) {
-        const int c = -R + bi * L;
-        const int p0 = c - R;
-        // ---- window [p0, p0 + 64) of every row into the tile ------------------
-        for (int row = 0; row < nreal; ++row) {
-            const float *src = base + (int64_t)row * ls;
-            float *dst = A + trow(row) * RF_TS;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int p = p0 + 32 * h + lane;
-                const bool v = (unsigned)p < (unsigned)n;
-                rf_cp4(dst + 32 * h + lane, v ? src + p : src, v);
+        const int c = -RH + bi * L4;  // first output, a multiple of 4
+        const int pa = c - RH;        // window start, a multiple of 4
+        // ---- window [pa, pa + 68) of every row, 16-byte chunks ---------------
+        {
+            int row = lane / 17, cc = lane - 17 * (lane / 17);
+            for (int k = lane; k < nreal * 17; k += 32) {
+                const int p = pa + 4 * cc;
+                const bool v = (unsigned)p < (unsigned)n;  // a chunk lies wholly inside or outside
+                const float *src = base + (int64_t)row * ls;
+                rf_cp16(A + rf_trow(row) * RF_TS + 4 * cc, v ? src + p : src, v);
+                cc += 15;
+                row += 1;
+                if (cc >= 17) {
+                    cc -= 17;
+                    row += 1;
+                }
             }
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         __syncwarp();
-        // ---- the previous block's held-back outputs (positions p0 .. p0 + R - 1,
-        // copied above as this window's first inputs) ---------------------------
-        if (bi > 0) {
-            for (int k = lane; k < R * 32; k += 32) {
-                const int q = k / R, i = k - q * R;
-                const int o = p0 + i;
-                if ((unsigned)o < (unsigned)n) {
-                    const float2 v = held[i][q];
-                    float *d = base + (int64_t)(2 * q) * ls + o;
-                    if (2 * q < nreal) d[0] = v.x;
-                    if (2 * q + 1 < nreal) d[ls] = v.y;
-                }
-            }
-        }
-        // ---- this lane's pair: FFT-64 in registers -----------------------------
+        // the previous block's held-back outputs are this window's first RH positions
+        if (bi > 0) put_held(pa);
+        // ---- this lane's pair: FFT-64 in registers ------------------------------
         float2 x[64];
         {
-            const float *ra = A + lane * RF_TS, *rb = A + (32 + lane) * RF_TS;
+            const float4 *ra = reinterpret_cast<const float4 *>(A + lane * RF_TS);
+            const float4 *rb = reinterpret_cast<const float4 *>(A + (32 + lane) * RF_TS);
 #pragma unroll
-            for (int i = 0; i < 64; ++i) x[i] = make_float2(ra[i], rb[i]);
+            for (int m = 0; m < 17; ++m) {
+                const float4 u = ra[m], w = rb[m];
+                const float ua[4] = {u.x, u.y, u.z, u.w}, wa[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int i = 4 * m + k - E;
+                    if (i >= 0 && i < 64) x[i] = make_float2(ua[k], wa[k]);
+                }
+            }
         }
         __syncwarp();  // every lane has its column: the tile is free for outputs
         if (!vb) {
@@ -478,7 +502,7 @@ __device__ __forceinline__ void rf_row_body(const OsJob &J, const OsTileInfo &T,
         if (masked) {
 #pragma unroll
             for (int i = 0; i < 64; ++i) {
-                const int p = p0 + i;
+                const int p = c - R + i;
                 const bool px = p >= xlo && p < xhi;
                 x[i].x = (in_a && px) ? x[i].x - b : 0.0f;
                 x[i].y = (in_b && px) ? x[i].y - b : 0.0f;
@@ -487,57 +511,43 @@ __device__ __forceinline__ void rf_row_body(const OsJob &J, const OsTileInfo &T,
         {
             float2 s2 = make_float2(0.0f, 0.0f);  // input mass: block outputs' positions
 #pragma unroll
-            for (int i = R; i < R + L; ++i) s2 = r_add(s2, x[i]);
+            for (int i = R; i < R + L4; ++i) s2 = r_add(s2, x[i]);
             acc_in += (double)(va ? s2.x : 0.0f) + (double)(vb ? s2.y : 0.0f);
         }
         r_fft64_fwd(x);
         r_modulate(x, hh);
         r_fft64_inv(x);
-        {
-            float *wa = A + lane * RF_TS, *wb = A + (32 + lane) * RF_TS;
 #pragma unroll
-            for (int i = R; i < R + L; ++i) {
-                const int o = c + i - R;
-                if ((unsigned)o < (unsigned)n) {
-                    if (i >= L) {
-                        held[i - L][lane] = x[i];
-                    } else {
-                        wa[i - R] = x[i].x;
-                        wb[i - R] = x[i].y;
-                    }
-                } else if (o >= -R && o < n + R) {
-                    lk = r_add(lk, x[i]);
-                }
+        for (int i = R; i < R + L4; ++i) {
+            const int o = c + i - R;
+            if (!((unsigned)o < (unsigned)n) && o >= -R && o < n + R) lk = r_add(lk, x[i]);
+        }
+        {
+            float4 *wa = reinterpret_cast<float4 *>(A + lane * RF_TS);
+            float4 *wb = reinterpret_cast<float4 *>(A + (32 + lane) * RF_TS);
+#pragma unroll
+            for (int m = 0; m < L4 / 4; ++m) {
+                wa[m] = make_float4(x[R + 4 * m].x, x[R + 4 * m + 1].x, x[R + 4 * m + 2].x, x[R + 4 * m + 3].x);
+                wb[m] = make_float4(x[R + 4 * m].y, x[R + 4 * m + 1].y, x[R + 4 * m + 2].y, x[R + 4 * m + 3].y);
             }
         }
         __syncwarp();
-        // ---- outputs [c, c + L - R) of every row, coalesced along x ------------
-        for (int row = 0; row < nreal; ++row) {
-            float *d = base + (int64_t)row * ls;
-            const float *sv = A + trow(row) * RF_TS;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int j = 32 * h + lane;
-                const int o = c + j;
-                if (j < L - R && (unsigned)o < (unsigned)n) d[o] = sv[j];
-            }
+        // ---- outputs [c, c + L4 - RH) of every row; the rest is held back ------
+        for (int k = lane; k < nreal * NST; k += 32) {
+            const int row = k / NST, cc = k - row * NST;
+            const int o = c + 4 * cc;
+            if ((unsigned)o < (unsigned)n)
+                *reinterpret_cast<float4 *>(base + (int64_t)row * ls + o) =
+                    *reinterpret_cast<const float4 *>(A + rf_trow(row) * RF_TS + 4 * cc);
+        }
+        for (int k = lane; k < nreal * NHD; k += 32) {
+            const int row = k / NHD, cc = k - row * NHD;
+            *reinterpret_cast<float4 *>(held + row * RH + 4 * cc) =
+                *reinterpret_cast<const float4 *>(A + rf_trow(row) * RF_TS + (L4 - RH) + 4 * cc);
         }
         __syncwarp();  // the tile is refilled by the next block
     }
-    // the last block's held-back outputs
-    {
-        const int clast = -R + (nblocks - 1) * L;
-        for (int k = lane; k < R * 32; k += 32) {
-            const int q = k / R, i = k - q * R;
-            const int o = clast + L - R + i;
-            if ((unsigned)o < (unsigned)n) {
-                const float2 v = held[i][q];
-                float *d = base + (int64_t)(2 * q) * ls + o;
-                if (2 * q < nreal) d[0] = v.x;
-                if (2 * q + 1 < nreal) d[ls] = v.y;
-            }
-        }
-    }
+    put_held(-RH + (nblocks - 1) * L4 + L4 - RH);
     double *mass = J.mass;
     const double s_in = r_warp_sum(acc_in);
     const double s_lk = r_warp_sum((double)(va ? lk.x : 0.0f) + (double)(vb ? lk.y : 0.0f));
@@ -551,8 +561,8 @@ __global__ void __launch_bounds__(32, 12) rf_row_kernel(const OsJob *__restrict_
                                                         const OsTileInfo *__restrict__ tiles)
 {
     __shared__ __align__(16) float A[64 * RF_TS];
+    __shared__ __align__(16) float held[64 * 8];  // held-back outputs [row][RH]
     __shared__ __align__(16) float2 hh[64];
-    __shared__ float2 held[RF_RMAX][32];  // held-back outputs [i][pair]
     const OsTileInfo T = tiles[blockIdx.x];
     const OsJob &J = jobs[T.job];
     hh[threadIdx.x] = J.HH[threadIdx.x];
@@ -576,7 +586,9 @@ static bool rf_row_enabled();
 bool rf_eligible(const OsJob &j)
 {
     if (j.r < 1 || j.r > RF_RMAX) return false;
-    if (j.kind == PASS_X) return rf_row_enabled();
+    if (j.kind == PASS_X)
+        return rf_row_enabled() && (j.n & 3) == 0 && (j.line_stride & 3) == 0 &&
+               (reinterpret_cast<uintptr_t>(j.data) & 15) == 0;
     return j.line_stride == 1;
 }
 
@@ -599,14 +611,13 @@ void rf_append_tiles(const OsJob &j, int job, std::vector<OsTileInfo> &out)
         }
 }
 
-// The x pass uses the register-FFT kernel only when VFD_RF_X=1 (the
-// overlap-save kernel is faster there).
+// VFD_RF_X=0 keeps the x pass on the overlap-save kernel.
 static bool rf_row_enabled()
 {
     static int on = -1;
     if (on < 0) {
         const char *e = getenv("VFD_RF_X");
-        on = (e && e[0] == '1') ? 1 : 0;
+        on = (e && e[0] == '0') ? 0 : 1;
     }
     return on == 1;
 }
