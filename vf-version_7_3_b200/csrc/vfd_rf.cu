@@ -151,6 +151,11 @@ __device__ __forceinline__ void r_modulate(float2 (&x)[64], const float2 *hh)
 // ---------------------------------------------------------------------------
 // y / z passes: one warp = one tile of 64 lines (32 pairs) of one outer index.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void rf_prefetch_l2(const void *p)
+{
+    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+}
+
 template <int R, bool V2>
 __device__ __forceinline__ void rf_col_body(const OsJob &J, const OsTileInfo &T, const float2 *hh,
                                             float2 (*held)[32])
@@ -167,8 +172,7 @@ __device__ __forceinline__ void rf_col_body(const OsJob &J, const OsTileInfo &T,
     const float keep = J.keep, b = J.b;
     const int nblocks = (n + 2 * R + L - 1) / L;
     // one output (or held-back output) of the pair at position o
-    auto put = [&](int o, float2 v) {
-        float *d = base + (int64_t)o * ps;
+    auto put = [&](float *d, float2 v) {
         if (V2) {
             *reinterpret_cast<float2 *>(d) = v;
         } else {
@@ -182,10 +186,16 @@ __device__ __forceinline__ void rf_col_body(const OsJob &J, const OsTileInfo &T,
         for (int bi = 0; bi < nblocks; ++bi) {
             const int c = -R + bi * L;  // first output of the block
             const int p0 = c - R;       // first input
+            const bool inner = p0 >= 0 && p0 + 64 <= n;  // window and outputs inside the line
+            float *const w0 = base + (int64_t)p0 * ps;
             float2 x[64];
             {
-                const float *sp = base + (int64_t)p0 * ps;
-                if (V2) {
+                const float *sp = w0;
+                if (inner) {
+#pragma unroll
+                    for (int i = 0; i < 64; ++i, sp += ps)
+                        x[i] = V2 ? *reinterpret_cast<const float2 *>(sp) : make_float2(sp[0], vb ? sp[1] : 0.0f);
+                } else if (V2) {
 #pragma unroll
                     for (int i = 0; i < 64; ++i, sp += ps)
                         x[i] = ((unsigned)(p0 + i) < (unsigned)n) ? *reinterpret_cast<const float2 *>(sp)
@@ -198,20 +208,27 @@ __device__ __forceinline__ void rf_col_body(const OsJob &J, const OsTileInfo &T,
                     }
                 }
             }
+            // the next block's new samples start for L2 while this one is transformed
+            if (bi + 1 < nblocks) {
+                const int q0 = p0 + 64, q1 = min(p0 + L + 64, n);
+                const float *pp = base + (int64_t)q0 * ps;
+                for (int q = q0; q < q1; ++q, pp += ps) rf_prefetch_l2(pp);
+            }
             // the previous block's held-back outputs: positions p0 .. p0 + R - 1,
             // just loaded above as this window's first inputs
             if (bi > 0) {
 #pragma unroll
                 for (int i = 0; i < R; ++i)
-                    if ((unsigned)(p0 + i) < (unsigned)n) put(p0 + i, held[i][lane]);
+                    if ((unsigned)(p0 + i) < (unsigned)n) put(w0 + (int64_t)i * ps, held[i][lane]);
             }
             r_fft64_fwd(x);
             r_modulate(x, hh);
             r_fft64_inv(x);
+            float *d = w0 + (int64_t)R * ps;  // position of sample R = first output c
 #pragma unroll
-            for (int i = R; i < R + L; ++i) {
+            for (int i = R; i < R + L; ++i, d += ps) {
                 const int o = c + i - R;
-                if ((unsigned)o < (unsigned)n) {
+                if (inner || (unsigned)o < (unsigned)n) {
                     float2 v = x[i];
                     if (zlast) {
                         cv = r_add(cv, v);
@@ -219,7 +236,7 @@ __device__ __forceinline__ void rf_col_body(const OsJob &J, const OsTileInfo &T,
                         ot = r_add(ot, v);
                     }
                     if (i >= L) held[i - L][lane] = v;  // stored after the next block's loads
-                    else put(o, v);
+                    else put(d, v);
                 } else if (o >= -R && o < n + R) {
                     lk = r_add(lk, x[i]);
                 }
@@ -230,7 +247,7 @@ __device__ __forceinline__ void rf_col_body(const OsJob &J, const OsTileInfo &T,
 #pragma unroll
         for (int i = 0; i < R; ++i) {
             const int o = clast + L - R + i;
-            if ((unsigned)o < (unsigned)n) put(o, held[i][lane]);
+            if ((unsigned)o < (unsigned)n) put(base + (int64_t)o * ps, held[i][lane]);
         }
     }
     double *mass = J.mass;
