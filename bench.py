@@ -30,10 +30,10 @@ for p in (os.path.join(ROOT, "vf-version_7_3_b200"), ROOT):
         sys.path.insert(0, p)
 
 METRIC = "voxel-steps/s"
-# ncu dram__bytes_read.sum + dram__bytes_write.sum per axis-pass launch of this
-# workload (8 fields of 512x256x384), scaled by voxels from the 512x256x128
-# capture in profiles/os_pass_pipe_512x256x128.md (3 x 1021 MB).
-AXIS_TRAFFIC_BYTES = 3.059e9
+# ncu dram__bytes_read.sum + dram__bytes_write.sum per y/z axis-pass launch of
+# this workload (8 fields of 512x256x384), scaled by voxels from the
+# 512x256x128 capture in profiles/rf_pass_512x256x128.md (3 x 1041 MB).
+AXIS_TRAFFIC_BYTES = 3.12e9
 
 
 def peaks():
@@ -446,7 +446,7 @@ def main():
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": AXIS_TRAFFIC_BYTES,
-                "kernel": "os_pass_kernel (x, y, z axis passes)",
+                "kernel": "rf_col_kernel (y, z) / rf_row_kernel (x): axis passes",
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
                 "peak_source": f"{peak_kind} hbm_gbs",
                 "share_of_step": axis_ms / ms if ms > 0 else None,
