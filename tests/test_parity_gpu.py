@@ -115,6 +115,29 @@ def test_constant_vf_padding_rule(gpu):
         check_mass(outs[f], mass[f], 1 - dec[f], float(np.float32(base[f])), nx * ny * nz)
 
 
+# The pass a world uses depends on its shape and radii: the register-FFT pass
+# for radius <= 8 (y/z with 8-byte pair accesses when nx is even, 4-byte
+# otherwise; x with 16-byte tiles when nx is a multiple of 4, else the
+# overlap-save x pass), the overlap-save pass for radius 9..16.  Tiles of 64
+# lines end partly filled and with an odd line count on these grids.
+PATH_GRIDS = [(96, 70, 33), (70, 33, 41), (37, 65, 29), (132, 9, 66)]
+SIGMAS_RF = [0.3, 0.6, 1.0, 1.3, 1.6, 2.0, 2.3, 2.6]   # radii 1..8
+SIGMAS_OS = [0.6, 3.2, 4.0]                            # radii 2, 10, 12
+
+
+@pytest.mark.parametrize("grid", PATH_GRIDS)
+@pytest.mark.parametrize("sigmas", [SIGMAS_RF, SIGMAS_OS], ids=["r1-8", "r2-12"])
+def test_pass_paths_against_oracle(gpu, grid, sigmas):
+    nx, ny, nz = grid
+    dec = [0.03] * len(sigmas)
+    inputs = configs.field_inputs(11, 2, grid, 64, n_fields=len(sigmas))
+    outs, mass, _ = run_world(grid, sigmas, dec, inputs, substeps=2)
+    for f, (u, idx, amt) in enumerate(inputs):
+        ref = oracle.tick(u, sigmas[f], dec[f], 2, idx, amt)
+        assert rel_l2(outs[f], ref) <= REL_L2, (grid, sigmas[f])
+        check_mass(outs[f], mass[f], 1 - dec[f], 0.0, nx * ny * nz)
+
+
 def test_constant_field_fixed_point(gpu):
     c = 5e-4
     grid = (40, 30, 20)
