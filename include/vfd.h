@@ -127,6 +127,46 @@ vfd_status vfd_world_fft_dims(const vfd_world *w, int *fft3);
 /* Device bytes this world holds. */
 vfd_status vfd_world_device_bytes(const vfd_world *w, size_t *bytes);
 
+/* ---- autotuning (VFD_METHOD_SEPARABLE worlds) ---------------------------
+ * Per axis, the pass that runs it: the register FFT (kernel radius <= 8),
+ * overlap-save FFT-64 blocks (radius <= 16) at 3 or 4 resident CTAs per SM,
+ * or a full-line FFT with a chosen padded length (the three cheapest
+ * 7-smooth lengths >= n + r), radix order and kernel variant.  The reference
+ * leaves the padded sizes to diffusion_helper::initChemDimensions
+ * (DiffusionHelper.cpp:381-461) and its transforms to cuFFT's planner. */
+typedef enum {
+    VFD_PASS_REGISTER_FFT = 0,
+    VFD_PASS_OVERLAP_SAVE = 1,
+    VFD_PASS_FULL_LINE = 2
+} vfd_pass_method;
+
+typedef struct vfd_axis_tuning {
+    int method;        /* vfd_pass_method                                */
+    int ctas_per_sm;   /* overlap-save: resident CTAs per SM (3 or 4)    */
+    int fft_len;       /* full line: padded FFT length                   */
+    int radix_order;   /* full line: 0 = radix 8 first, 1 = radix 4 first */
+    int variant;       /* full line: kernel variant (tile shape)         */
+    float ms;          /* tuned time of the pass over every field, or 0  */
+} vfd_axis_tuning;
+
+/* Times every candidate of each axis on temporary worlds of desc's shape
+ * (zero fields, `reps` timed launches each after one warm-up; the device
+ * needs room for one extra world), caches the fastest per shape (device,
+ * grid, padding rule, per-field radii) and writes it to out[3].  Later
+ * vfd_world_create calls with that shape use the cached choice; with the
+ * environment variable VFD_AUTOTUNE=1 they tune an uncached shape first. */
+vfd_status vfd_autotune(const vfd_world_desc *desc, int device, int reps, vfd_axis_tuning *out3);
+/* The pass each axis of this world runs (ms: the tuned time, 0 if the
+ * world was not created from a tuned choice). */
+vfd_status vfd_world_tuning(const vfd_world *w, vfd_axis_tuning *out3);
+/* Stores a choice for desc's shape in the cache (a saved tuning, or a pinned
+ * pass): later worlds of the shape run it.  An axis whose world cannot run
+ * the stored method (register FFT beyond radius 8 or on an unaligned x
+ * line, overlap-save beyond radius 16) falls back to the default pass. */
+vfd_status vfd_autotune_set(const vfd_world_desc *desc, int device, const vfd_axis_tuning *in3);
+/* Empties the per-shape cache. */
+vfd_status vfd_autotune_clear(void);
+
 /* ---- field transfer (H2D / D2H, Diffusion.cu:72-122) ------------------ */
 vfd_status vfd_upload_field(vfd_world *w, int field, const float *host, void *stream);
 vfd_status vfd_download_field(vfd_world *w, int field, float *host, void *stream);

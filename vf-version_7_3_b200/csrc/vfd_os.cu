@@ -659,6 +659,8 @@ static int os_min_blocks()
     return m;
 }
 
+int os_default_ctas_per_sm() { return os_min_blocks(); }
+
 template <bool XP, int MINB>
 static cudaError_t launch_os_t(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int rmin, cudaStream_t st)
 {
@@ -695,7 +697,8 @@ static cudaError_t launch_os_t(const OsJob *jobs, const OsTileInfo *tiles, int n
     return cudaGetLastError();
 }
 
-cudaError_t launch_os(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int rmin, int axis, cudaStream_t st)
+cudaError_t launch_os(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int rmin, int axis, cudaStream_t st,
+                      int ctas_per_sm)
 {
     if (ntiles <= 0) return cudaSuccess;
     int dev = 0;
@@ -707,7 +710,7 @@ cudaError_t launch_os(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, in
         ready = dev >= 0 && dev < 64 && g_tw_done[dev];
     }
     if (!ready && (e = os_prepare()) != cudaSuccess) return e;
-    if (os_min_blocks() == 4) {
+    if ((ctas_per_sm > 0 ? ctas_per_sm : os_min_blocks()) == 4) {
         if (axis == PASS_X) return launch_os_t<true, 4>(jobs, tiles, ntiles, rmin, st);
         return launch_os_t<false, 4>(jobs, tiles, ntiles, rmin, st);
     }

@@ -62,8 +62,13 @@ void os_append_tiles(const OsJob &j, int job, std::vector<OsTileInfo> &out);
 cudaError_t os_prepare();
 // Dynamic shared memory of a launch whose jobs have radius >= rmin.
 size_t os_smem_bytes(int rmin, int axis);
+// Resident CTAs per SM a launch uses when none is asked for.
+int os_default_ctas_per_sm();
 // One persistent launch over `ntiles` tiles (tiles[i]) of jobs that all
 // belong to `axis` and have radius >= rmin.
-cudaError_t launch_os(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int rmin, int axis, cudaStream_t st);
+// ctas_per_sm: resident CTAs per SM the kernel is compiled for (3 or 4; 0:
+// the default, 3, or VFD_OS_MINB=4).
+cudaError_t launch_os(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int rmin, int axis, cudaStream_t st,
+                      int ctas_per_sm = 0);
 
 }  // namespace vfd

@@ -15,6 +15,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -38,11 +40,17 @@ static thread_local std::string g_thread_error = "";
 // snapTransformSize, Diffusion.cu:39-70).  Among 7-smooth lengths the cheapest
 // by a per-stage cost model is taken; radices 8,7,5,4,3,2.
 // ---------------------------------------------------------------------------
-static bool make_plan(int F, FftPlan *p)
+// Radix orders for the Stockham stages: 0 takes radix 8 first, 1 radix 4
+// (more, cheaper stages); the autotuner times both.
+constexpr int kPlanOrders = 2;
+
+static bool make_plan_order(int F, int order_id, FftPlan *p)
 {
     int n = F, k = 0;
-    static const int order[] = {8, 7, 5, 4, 3, 2};
-    for (int r : order) {
+    static const int orders[kPlanOrders][6] = {{8, 7, 5, 4, 3, 2}, {4, 7, 5, 8, 3, 2}};
+    const int *order = orders[(order_id >= 0 && order_id < kPlanOrders) ? order_id : 0];
+    for (int i = 0; i < 6; ++i) {
+        const int r = order[i];
         while (n % r == 0) {
             if (k >= MAX_STAGES) return false;
             p->radix[k++] = r;
@@ -61,6 +69,8 @@ static bool make_plan(int F, FftPlan *p)
     }
     return true;
 }
+
+static bool make_plan(int F, FftPlan *p) { return make_plan_order(F, 0, p); }
 
 static bool variant_fits(int v, const FftPlan &p)
 {
@@ -266,6 +276,10 @@ struct vfd_world {
     OsTileInfo *d_os_tiles[3] = {nullptr, nullptr, nullptr};    // all-field launches
     OsTileInfo *d_os_ftiles[3] = {nullptr, nullptr, nullptr};   // single-field launches, [field][tiles]
     bool use_rf[3] = {false, false, false};       // register-FFT pass (radius <= RF_RMAX)
+    bool allow_rf[3] = {true, true, true};        // tuning may keep an axis off the register-FFT pass
+    int os_minb[3] = {0, 0, 0};                   // overlap-save CTAs per SM (0: default)
+    int plan_order[3] = {0, 0, 0};                // full-line radix order
+    float tuned_ms[3] = {0.0f, 0.0f, 0.0f};       // tuned pass times (0: not tuned)
     std::vector<RfGroup> rf[3];                   // all-field launches
     std::vector<std::vector<RfGroup>> rf_field[3];  // single-field launches
 
@@ -526,7 +540,84 @@ const char *vfd_last_error(const vfd_world *w)
 
 uint64_t vfd_kernel_launch_count(void) { return g_launches.load(); }
 
+// ---------------------------------------------------------------------------
+// Autotuning: per axis, the pass (register FFT, overlap-save at 3 or 4 CTAs
+// per SM, full-line Stockham with a chosen FFT length, radix order and kernel
+// variant), timed on a temporary world of the same shape and cached per
+// shape; vfd_world_create applies a cached choice.
+// ---------------------------------------------------------------------------
+enum { PASS_METHOD_AUTO = -1, PASS_METHOD_RF = 0, PASS_METHOD_OS = 1, PASS_METHOD_FULL = 2 };
+
+struct AxisChoice {
+    int method = PASS_METHOD_AUTO;
+    int minb = 0;      // overlap-save CTAs per SM
+    int F = 0;         // full line: FFT length
+    int order = 0;     // full line: radix order
+    int variant = -1;  // full line: kernel variant
+    float ms = 0.0f;
+};
+struct ShapeChoice {
+    AxisChoice ax[3];
+};
+
+static std::mutex g_tune_mu;
+static std::map<std::string, ShapeChoice> g_tune_cache;
+
+// Cache key: device, grid, padding rule and every field's radius per axis.
+static std::string shape_key(const vfd_world_desc *d, int device)
+{
+    std::string k = std::to_string(device) + ":" + std::to_string(d->nx) + "x" + std::to_string(d->ny) + "x" +
+                    std::to_string(d->nz) + ":p" + std::to_string(d->pad_mode) + ":e" +
+                    std::to_string(d->pad_mode == VFD_PAD_CONSTANT_VF ? d->epi_boundary : 0) + ":m" +
+                    std::to_string(d->method) + ":r";
+    for (int f = 0; f < d->n_fields; ++f)
+        for (int a = 0; a < 3; ++a) {
+            int r = d->fields[f].radius[a];
+            if (r <= 0) r = (int)std::ceil(3.0 * d->fields[f].sigma[a]);
+            k += std::to_string(r) + ",";
+        }
+    return k;
+}
+
+static bool cached_choice(const vfd_world_desc *d, int device, ShapeChoice *out)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(shape_key(d, device));
+    if (it == g_tune_cache.end()) return false;
+    *out = it->second;
+    return true;
+}
+
+static vfd_status world_create(const vfd_world_desc *d, int device, const ShapeChoice *ch, vfd_world **out);
+static vfd_status tune_shape(const vfd_world_desc *d, int device, int reps, ShapeChoice *out);
+
+static bool autotune_on_create()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("VFD_AUTOTUNE");
+        on = (e && e[0] == '1') ? 1 : 0;
+    }
+    return on == 1;
+}
+
 vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out)
+{
+    if (!out) return fail(nullptr, VFD_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    if (!d || !d->fields) return fail(nullptr, VFD_ERR_INVALID_ARG, "desc or desc->fields is NULL");
+    ShapeChoice ch;
+    bool have = d->method == VFD_METHOD_SEPARABLE && cached_choice(d, device, &ch);
+    if (!have && d->method == VFD_METHOD_SEPARABLE && autotune_on_create() && d->nx >= 1 && d->ny >= 1 &&
+        d->nz >= 1 && d->n_fields >= 1 && tune_shape(d, device, 3, &ch) == VFD_OK) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[shape_key(d, device)] = ch;
+        have = true;
+    }
+    return world_create(d, device, have ? &ch : nullptr, out);
+}
+
+static vfd_status world_create(const vfd_world_desc *d, int device, const ShapeChoice *ch, vfd_world **out)
 {
     if (!out) return fail(nullptr, VFD_ERR_INVALID_ARG, "out is NULL");
     *out = nullptr;
@@ -575,6 +666,8 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
     }
     for (int a = 0; a < 3; ++a) {
         int F = d->fft[a];
+        const int order = ch ? ch->ax[a].order : 0;
+        if (F <= 0 && ch && ch->ax[a].F >= dims[a] + rmax[a]) F = ch->ax[a].F;
         if (F > 0) {
             if (F < dims[a] + rmax[a]) {
                 delete w;
@@ -584,10 +677,11 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
                 delete w;
                 return fail(nullptr, VFD_ERR_INVALID_ARG, "the general 3D methods need an even x FFT length");
             }
-            if (!make_plan(F, &w->plan[a]) || !any_variant_fits(w->plan[a])) {
+            if (!make_plan_order(F, order, &w->plan[a]) || !any_variant_fits(w->plan[a])) {
                 delete w;
                 return fail(nullptr, VFD_ERR_NOT_SUPPORTED, "fft length not 7-smooth or too long");
             }
+            w->plan_order[a] = order;
         } else {
             F = choose_fft_len(dims[a], rmax[a], general && a == 0);
             if (F < 0) {
@@ -595,10 +689,18 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
                 return fail(nullptr, VFD_ERR_NOT_SUPPORTED, "axis too long for the shared-memory FFT");
             }
             make_plan(F, &w->plan[a]);
+            FftPlan q;
+            if (order != 0 && make_plan_order(F, order, &q) && any_variant_fits(q)) {
+                w->plan[a] = q;
+                w->plan_order[a] = order;
+            }
         }
         w->F[a] = F;
         w->Fmax = std::max(w->Fmax, F);
         w->variant[a] = pick_variant(std::vector<FftPlan>{w->plan[a]});
+        if (ch && ch->ax[a].variant >= 0 && ch->ax[a].variant < kNumAxisVariants &&
+            variant_fits(ch->ax[a].variant, w->plan[a]))
+            w->variant[a] = ch->ax[a].variant;
     }
     for (int a = 0; a < 3; ++a) {
         if (w->variant[a] < 0) {
@@ -615,6 +717,13 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
             w->rmin[a] = rmn;
         }
     }
+    if (ch && !general)
+        for (int a = 0; a < 3; ++a) {
+            if (ch->ax[a].method == PASS_METHOD_FULL) w->use_os[a] = false;
+            if (ch->ax[a].method == PASS_METHOD_OS || ch->ax[a].method == PASS_METHOD_FULL) w->allow_rf[a] = false;
+            w->os_minb[a] = ch->ax[a].minb;
+            w->tuned_ms[a] = ch->ax[a].ms;
+        }
     if (general) {
         w->Fxh = w->F[0] / 2 + 1;
         w->gvar[0] = w->variant[0];
@@ -705,7 +814,7 @@ vfd_status vfd_world_create(const vfd_world_desc *d, int device, vfd_world **out
                 return bail(e, "os tiles");
         }
         for (int a = 0; a < 3 && rf_enabled(); ++a) {
-            bool ok = w->use_os[a];
+            bool ok = w->use_os[a] && w->allow_rf[a];
             for (int f = 0; f < w->nf; ++f) ok = ok && rf_eligible(oj[(size_t)a * w->nf + f]);
             if (!ok) continue;
             if ((e = rf_prepare()) != cudaSuccess) return bail(e, "register-FFT twiddles");
@@ -1138,6 +1247,37 @@ static vfd_status enqueue_general_substep(vfd_world *w, int f, cudaStream_t st)
 }
 
 // Enqueues n_substeps of one field (field >= 0) or of all fields (field < 0).
+// One axis pass of every field (field < 0) or of one field, with the pass
+// the world uses for that axis.
+static vfd_status enqueue_axis(vfd_world *w, int a, int field, cudaStream_t st)
+{
+    const int nj = field < 0 ? w->nf : 1;
+    if (w->use_rf[a]) {
+        if (field < 0)
+            VFD_CUDA(w, launch_rf_groups(w->d_osjobs + a * w->nf, w->rf[a], a, st));
+        else
+            VFD_CUDA(w, launch_rf_groups(w->d_osjobs + 3 * w->nf + a * w->nf + field, w->rf_field[a][field], a, st));
+    } else if (w->use_os[a]) {
+        const OsJob *jobs = field < 0 ? w->d_osjobs + a * w->nf : w->d_osjobs + 3 * w->nf + a * w->nf + field;
+        int tiles = 0;
+        if (field < 0)
+            for (int f = 0; f < w->nf; ++f) tiles += w->os_tiles[a][f];
+        else
+            tiles = w->os_tiles[a][field];
+        const OsTileInfo *ti = w->d_os_tiles[a];
+        if (field >= 0) {
+            ti = w->d_os_ftiles[a];
+            for (int f = 0; f < field; ++f) ti += w->os_tiles[a][f];
+        }
+        VFD_CUDA(w, launch_os(jobs, ti, tiles, w->rmin[a], a, st, w->os_minb[a]));
+    } else {
+        const AxisJob *jobs = field < 0 ? w->d_jobs + a * w->nf : w->d_jobs + 3 * w->nf + a * w->nf + field;
+        const int tiles = w->tiles_per_field[a] * nj;
+        VFD_CUDA(w, launch_axis(w->variant[a], jobs, nj, tiles, w->F[a], st));
+    }
+    return VFD_OK;
+}
+
 static vfd_status enqueue_tick(vfd_world *w, int field, int n_substeps, cudaStream_t st)
 {
     if (w->method != VFD_METHOD_SEPARABLE) {
@@ -1158,7 +1298,6 @@ static vfd_status enqueue_tick(vfd_world *w, int field, int n_substeps, cudaStre
         }
         return VFD_OK;
     }
-    const int nj = field < 0 ? w->nf : 1;
     for (int s = 0; s < n_substeps; ++s) {
         if (field < 0)
             VFD_CUDA(w, cudaMemsetAsync(w->d_mass, 0, sizeof(double) * MS_COUNT * w->nf, st));
@@ -1166,31 +1305,8 @@ static vfd_status enqueue_tick(vfd_world *w, int field, int n_substeps, cudaStre
             VFD_CUDA(w, cudaMemsetAsync(w->d_mass + (int64_t)field * MS_COUNT, 0, sizeof(double) * MS_COUNT, st));
         for (int a = 0; a < 3; ++a) {
             LaunchTimer lt(w, a, st);
-            if (w->use_rf[a]) {
-                if (field < 0)
-                    VFD_CUDA(w, launch_rf_groups(w->d_osjobs + a * w->nf, w->rf[a], a, st));
-                else
-                    VFD_CUDA(w, launch_rf_groups(w->d_osjobs + 3 * w->nf + a * w->nf + field, w->rf_field[a][field],
-                                                 a, st));
-            } else if (w->use_os[a]) {
-                const OsJob *jobs =
-                    field < 0 ? w->d_osjobs + a * w->nf : w->d_osjobs + 3 * w->nf + a * w->nf + field;
-                int tiles = 0;
-                if (field < 0)
-                    for (int f = 0; f < w->nf; ++f) tiles += w->os_tiles[a][f];
-                else
-                    tiles = w->os_tiles[a][field];
-                const OsTileInfo *ti = w->d_os_tiles[a];
-                if (field >= 0) {
-                    ti = w->d_os_ftiles[a];
-                    for (int f = 0; f < field; ++f) ti += w->os_tiles[a][f];
-                }
-                VFD_CUDA(w, launch_os(jobs, ti, tiles, w->rmin[a], a, st));
-            } else {
-                const AxisJob *jobs = field < 0 ? w->d_jobs + a * w->nf : w->d_jobs + 3 * w->nf + a * w->nf + field;
-                const int tiles = w->tiles_per_field[a] * nj;
-                VFD_CUDA(w, launch_axis(w->variant[a], jobs, nj, tiles, w->F[a], st));
-            }
+            vfd_status r = enqueue_axis(w, a, field, st);
+            if (r != VFD_OK) return r;
             lt.done();
         }
     }
@@ -1277,6 +1393,267 @@ vfd_status vfd_sample_field(vfd_world *w, int field, int stride, float scale, fl
     return VFD_OK;
 }
 
+// ---- autotuning -------------------------------------------------------------
+// The `k` cheapest FFT lengths (plan_cost order) for a line of n with radius r.
+static int fft_len_candidates(int n, int r, int k, int *out)
+{
+    std::vector<std::pair<double, int>> c;
+    const int lo = n + r;
+    for (int F = lo; F <= 2 * lo + 16; ++F) {
+        FftPlan p;
+        if (!make_plan(F, &p) || !any_variant_fits(p)) continue;
+        c.push_back({plan_cost(p), F});
+    }
+    std::stable_sort(c.begin(), c.end(), [](const std::pair<double, int> &x, const std::pair<double, int> &y) {
+        return x.first < y.first;
+    });
+    const int m = std::min(k, (int)c.size());
+    for (int i = 0; i < m; ++i) out[i] = c[i].second;
+    return m;
+}
+
+static bool same_radices(const FftPlan &p, const FftPlan &q)
+{
+    if (p.nst != q.nst) return false;
+    for (int s = 0; s < p.nst; ++s)
+        if (p.radix[s] != q.radix[s]) return false;
+    return true;
+}
+
+// Mean time of one pass of axis a over every field (ms), or < 0 on error.
+static float time_axis(vfd_world *w, int a, int reps, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1)
+{
+    if (enqueue_axis(w, a, -1, st) != VFD_OK) return -1.0f;
+    if (cudaEventRecord(e0, st) != cudaSuccess) return -1.0f;
+    for (int i = 0; i < reps; ++i)
+        if (enqueue_axis(w, a, -1, st) != VFD_OK) return -1.0f;
+    if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) return -1.0f;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) return -1.0f;
+    return ms / reps;
+}
+
+// Times the candidates of each axis on worlds built from `proto` and keeps
+// the fastest in best (candidates whose world does not run the asked pass
+// on an axis are not timed there).
+struct TuneRun {
+    const vfd_world_desc *d;
+    int device, reps;
+    cudaStream_t st;
+    cudaEvent_t e0, e1;
+    ShapeChoice best;
+    bool have[3] = {false, false, false};
+};
+
+static vfd_status tune_candidate(TuneRun &T, const ShapeChoice &proto, const bool *axes)
+{
+    vfd_world *w = nullptr;
+    vfd_status s = world_create(T.d, T.device, &proto, &w);
+    if (s == VFD_ERR_NOT_SUPPORTED || s == VFD_ERR_OUT_OF_MEMORY) return VFD_OK;  // candidate does not fit
+    if (s != VFD_OK) return s;
+    for (int a = 0; a < 3 && s == VFD_OK; ++a) {
+        if (!axes[a]) continue;
+        const AxisChoice &c = proto.ax[a];
+        int method = w->use_rf[a] ? PASS_METHOD_RF : w->use_os[a] ? PASS_METHOD_OS : PASS_METHOD_FULL;
+        if (c.method != PASS_METHOD_AUTO && method != c.method) continue;
+        if (method == PASS_METHOD_FULL && c.variant >= 0 && w->variant[a] != c.variant) continue;
+        const float ms = time_axis(w, a, T.reps, T.st, T.e0, T.e1);
+        if (ms < 0.0f) {
+            s = VFD_ERR_CUDA;
+            break;
+        }
+        if (!T.have[a] || ms < T.best.ax[a].ms) {
+            AxisChoice b;
+            b.method = method;
+            b.minb = method == PASS_METHOD_OS ? (c.minb > 0 ? c.minb : os_default_ctas_per_sm()) : 0;
+            b.F = method == PASS_METHOD_FULL ? w->F[a] : 0;
+            b.order = method == PASS_METHOD_FULL ? w->plan_order[a] : 0;
+            b.variant = method == PASS_METHOD_FULL ? w->variant[a] : -1;
+            b.ms = ms;
+            T.best.ax[a] = b;
+            T.have[a] = true;
+        }
+    }
+    vfd_world_destroy(w);
+    return s;
+}
+
+static vfd_status tune_shape(const vfd_world_desc *d, int device, int reps, ShapeChoice *out)
+{
+    if (!d || !d->fields || d->n_fields < 1 || d->nx < 1 || d->ny < 1 || d->nz < 1)
+        return fail(nullptr, VFD_ERR_INVALID_ARG, "invalid world description");
+    if (d->method != VFD_METHOD_SEPARABLE)
+        return fail(nullptr, VFD_ERR_NOT_SUPPORTED, "autotuning covers VFD_METHOD_SEPARABLE worlds");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(nullptr, VFD_ERR_NO_DEVICE, "no CUDA device visible");
+    if (device < 0 || device >= ndev) return fail(nullptr, VFD_ERR_INVALID_ARG, "device ordinal out of range");
+    DeviceGuard g(device);
+    TuneRun T;
+    T.d = d;
+    T.device = device;
+    T.reps = std::max(1, std::min(reps, 100));
+    if (cudaStreamCreateWithFlags(&T.st, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(nullptr, VFD_ERR_CUDA, "autotune: stream");
+    cudaEventCreate(&T.e0);
+    cudaEventCreate(&T.e1);
+    const bool all[3] = {true, true, true};
+    const int dims[3] = {d->nx, d->ny, d->nz};
+    int rmax[3] = {0, 0, 0};
+    for (int f = 0; f < d->n_fields; ++f)
+        for (int a = 0; a < 3; ++a) {
+            int r = d->fields[f].radius[a];
+            if (r <= 0) r = (int)std::ceil(3.0 * d->fields[f].sigma[a]);
+            rmax[a] = std::max(rmax[a], r);
+        }
+    vfd_status s = VFD_OK;
+    // register FFT (where the world would take it)
+    {
+        ShapeChoice c;
+        for (int a = 0; a < 3; ++a) c.ax[a].method = PASS_METHOD_RF;
+        s = tune_candidate(T, c, all);
+    }
+    // overlap-save at 3 and 4 resident CTAs per SM
+    for (int minb = 3; minb <= 4 && s == VFD_OK; ++minb) {
+        ShapeChoice c;
+        for (int a = 0; a < 3; ++a) {
+            c.ax[a].method = PASS_METHOD_OS;
+            c.ax[a].minb = minb;
+        }
+        s = tune_candidate(T, c, all);
+    }
+    // full line: FFT length x radix order x kernel variant; the FFT length of
+    // an axis that has fewer candidates stays at its cheapest
+    int cand[3][3], ncand[3];
+    for (int a = 0; a < 3; ++a) ncand[a] = d->fft[a] > 0 ? 0 : fft_len_candidates(dims[a], rmax[a], 3, cand[a]);
+    for (int k = 0; k < 3 && s == VFD_OK; ++k)
+        for (int order = 0; order < kPlanOrders && s == VFD_OK; ++order)
+            for (int v = 0; v < kNumAxisVariants && s == VFD_OK; ++v) {
+                ShapeChoice c;
+                bool axes[3] = {false, false, false}, any = false;
+                for (int a = 0; a < 3; ++a) {
+                    c.ax[a].method = PASS_METHOD_FULL;
+                    c.ax[a].order = order;
+                    c.ax[a].variant = v;
+                    const int F = d->fft[a] > 0 ? d->fft[a] : (ncand[a] > 0 ? cand[a][std::min(k, ncand[a] - 1)] : 0);
+                    c.ax[a].F = d->fft[a] > 0 ? 0 : F;
+                    if (F <= 0 || (k > 0 && k >= ncand[a])) continue;
+                    FftPlan p, p0;
+                    if (!make_plan_order(F, order, &p) || !variant_fits(v, p)) continue;
+                    if (order > 0 && make_plan_order(F, 0, &p0) && same_radices(p, p0)) continue;
+                    axes[a] = any = true;
+                }
+                if (any) s = tune_candidate(T, c, axes);
+            }
+    cudaEventDestroy(T.e0);
+    cudaEventDestroy(T.e1);
+    cudaStreamDestroy(T.st);
+    if (s != VFD_OK) return s;
+    for (int a = 0; a < 3; ++a)
+        if (!T.have[a]) return fail(nullptr, VFD_ERR_NOT_SUPPORTED, "autotune: no pass runs this shape");
+    *out = T.best;
+    return VFD_OK;
+}
+
+static void to_public(const AxisChoice &c, vfd_axis_tuning *o)
+{
+    o->method = c.method == PASS_METHOD_RF   ? VFD_PASS_REGISTER_FFT
+                : c.method == PASS_METHOD_OS ? VFD_PASS_OVERLAP_SAVE
+                                             : VFD_PASS_FULL_LINE;
+    o->ctas_per_sm = c.minb;
+    o->fft_len = c.F;
+    o->radix_order = c.order;
+    o->variant = c.variant;
+    o->ms = c.ms;
+}
+
+vfd_status vfd_autotune(const vfd_world_desc *desc, int device, int reps, vfd_axis_tuning *out3)
+{
+    if (!out3) return fail(nullptr, VFD_ERR_INVALID_ARG, "out3 is NULL");
+    ShapeChoice ch;
+    vfd_status s = tune_shape(desc, device, reps, &ch);
+    if (s != VFD_OK) return s;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[shape_key(desc, device)] = ch;
+    }
+    for (int a = 0; a < 3; ++a) to_public(ch.ax[a], &out3[a]);
+    return VFD_OK;
+}
+
+vfd_status vfd_world_tuning(const vfd_world *w, vfd_axis_tuning *out3)
+{
+    if (!w || !out3) return VFD_ERR_INVALID_ARG;
+    if (w->method != VFD_METHOD_SEPARABLE) return VFD_ERR_NOT_SUPPORTED;
+    for (int a = 0; a < 3; ++a) {
+        AxisChoice c;
+        c.method = w->use_rf[a] ? PASS_METHOD_RF : w->use_os[a] ? PASS_METHOD_OS : PASS_METHOD_FULL;
+        c.minb = c.method == PASS_METHOD_OS ? (w->os_minb[a] > 0 ? w->os_minb[a] : os_default_ctas_per_sm()) : 0;
+        c.F = c.method == PASS_METHOD_FULL ? w->F[a] : 0;
+        c.order = c.method == PASS_METHOD_FULL ? w->plan_order[a] : 0;
+        c.variant = c.method == PASS_METHOD_FULL ? w->variant[a] : -1;
+        c.ms = w->tuned_ms[a];
+        to_public(c, &out3[a]);
+    }
+    return VFD_OK;
+}
+
+vfd_status vfd_autotune_set(const vfd_world_desc *desc, int device, const vfd_axis_tuning *in3)
+{
+    if (!desc || !desc->fields || !in3 || desc->n_fields < 1)
+        return fail(nullptr, VFD_ERR_INVALID_ARG, "desc, desc->fields or in3 is NULL");
+    if (desc->method != VFD_METHOD_SEPARABLE)
+        return fail(nullptr, VFD_ERR_NOT_SUPPORTED, "tunings cover VFD_METHOD_SEPARABLE worlds");
+    const int dims[3] = {desc->nx, desc->ny, desc->nz};
+    ShapeChoice ch;
+    for (int a = 0; a < 3; ++a) {
+        const vfd_axis_tuning &t = in3[a];
+        AxisChoice &c = ch.ax[a];
+        if (t.method < VFD_PASS_REGISTER_FFT || t.method > VFD_PASS_FULL_LINE)
+            return fail(nullptr, VFD_ERR_INVALID_ARG, "unknown pass method");
+        c.method = t.method == VFD_PASS_REGISTER_FFT ? PASS_METHOD_RF
+                   : t.method == VFD_PASS_OVERLAP_SAVE ? PASS_METHOD_OS
+                                                        : PASS_METHOD_FULL;
+        c.ms = t.ms;
+        if (c.method == PASS_METHOD_OS) {
+            if (t.ctas_per_sm != 0 && t.ctas_per_sm != 3 && t.ctas_per_sm != 4)
+                return fail(nullptr, VFD_ERR_INVALID_ARG, "ctas_per_sm must be 0, 3 or 4");
+            c.minb = t.ctas_per_sm;
+        }
+        if (c.method == PASS_METHOD_FULL) {
+            if (t.radix_order < 0 || t.radix_order >= kPlanOrders)
+                return fail(nullptr, VFD_ERR_INVALID_ARG, "radix_order out of range");
+            if (t.variant < -1 || t.variant >= kNumAxisVariants)
+                return fail(nullptr, VFD_ERR_INVALID_ARG, "variant out of range");
+            int rmax = 0;
+            for (int f = 0; f < desc->n_fields; ++f) {
+                int r = desc->fields[f].radius[a];
+                if (r <= 0) r = (int)std::ceil(3.0 * desc->fields[f].sigma[a]);
+                rmax = std::max(rmax, r);
+            }
+            FftPlan p;
+            if (t.fft_len != 0 && (t.fft_len < dims[a] + rmax || !make_plan_order(t.fft_len, t.radix_order, &p) ||
+                                   !any_variant_fits(p)))
+                return fail(nullptr, VFD_ERR_INVALID_ARG, "fft_len is shorter than n + radius or has no plan");
+            if (t.fft_len != 0 && t.variant >= 0 && !variant_fits(t.variant, p))
+                return fail(nullptr, VFD_ERR_INVALID_ARG, "the kernel variant does not fit fft_len");
+            c.F = t.fft_len;
+            c.order = t.radix_order;
+            c.variant = t.variant;
+        }
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[shape_key(desc, device)] = ch;
+    return VFD_OK;
+}
+
+vfd_status vfd_autotune_clear(void)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache.clear();
+    return VFD_OK;
+}
+
 vfd_status vfd_world_set_profiling(vfd_world *w, int enable)
 {
     if (!w) return VFD_ERR_INVALID_ARG;
@@ -1355,6 +1732,7 @@ struct vfd_batch {
     OsJob *d_osjobs = nullptr;  // [3][njobs]
     int os_tiles[3] = {0, 0, 0};
     OsTileInfo *d_os_tiles[3] = {nullptr, nullptr, nullptr};
+    int os_minb[3] = {0, 0, 0};
     bool use_rf[3] = {false, false, false};
     std::vector<RfGroup> rf[3];
     cudaStream_t st = nullptr;
@@ -1412,6 +1790,7 @@ static cudaError_t batch_rf_setup(vfd_batch *b, const std::vector<OsJob> &oj)
     for (int a = 0; a < 3; ++a) {
         if (!b->use_os[a]) continue;
         bool ok = true;
+        for (auto *w : b->worlds) ok = ok && w->allow_rf[a];
         for (int i = 0; i < b->njobs; ++i) ok = ok && rf_eligible(oj[(size_t)a * b->njobs + i]);
         if (!ok) continue;
         cudaError_t e = rf_prepare();
@@ -1472,6 +1851,9 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
         }
         b->use_os[a] = all;
         b->rmin[a] = rmn;
+        b->os_minb[a] = b->worlds[0]->os_minb[a];
+        for (auto *w : b->worlds)
+            if (w->os_minb[a] != b->os_minb[a]) b->os_minb[a] = 0;
     }
     if (b->use_os[0] || b->use_os[1] || b->use_os[2]) {
         for (int a = 0; a < 3; ++a) {
@@ -1535,7 +1917,7 @@ static vfd_status batch_enqueue(vfd_batch *b, int n_substeps)
                 VFD_BCUDA(b, launch_rf_groups(b->d_osjobs + a * b->njobs, b->rf[a], a, b->st));
             else if (b->use_os[a])
                 VFD_BCUDA(b, launch_os(b->d_osjobs + a * b->njobs, b->d_os_tiles[a], b->os_tiles[a], b->rmin[a], a,
-                                       b->st));
+                                       b->st, b->os_minb[a]));
             else
                 VFD_BCUDA(b, launch_axis(b->variant[a], b->d_jobs + a * b->njobs, b->njobs, b->tiles[a],
                                          b->Fmax[a], b->st));

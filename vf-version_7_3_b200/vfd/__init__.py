@@ -44,7 +44,10 @@ EXPORTED = [
     "vfd_server_create", "vfd_server_submit", "vfd_server_wait", "vfd_server_drain",
     "vfd_server_get_stats", "vfd_server_clock", "vfd_server_destroy",
     "vfd_fft_diffuse3d_noalloc", "vfd_update_gradients", "vfd_sample_field", "vfd_write_vtk",
+    "vfd_autotune", "vfd_world_tuning", "vfd_autotune_set", "vfd_autotune_clear",
 ]
+
+PASS_METHODS = {0: "register_fft", 1: "overlap_save", 2: "full_line"}
 
 
 class VfdError(RuntimeError):
@@ -101,6 +104,16 @@ class ServerStats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class AxisTuning(C.Structure):
+    _fields_ = [("method", C.c_int), ("ctas_per_sm", C.c_int), ("fft_len", C.c_int),
+                ("radix_order", C.c_int), ("variant", C.c_int), ("ms", C.c_float)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["method"] = PASS_METHODS.get(self.method, self.method)
+        return d
 
 
 def load(path=LIB_PATH):
@@ -207,6 +220,52 @@ def field_params(sigma, decay_rate, radius=None, baseline=0.0):
     return p
 
 
+def _world_desc(nx, ny, nz, params, pad_mode, epi_boundary, fft, method):
+    """WorldDesc and the FieldParams array it points to (keep both alive)."""
+    arr = (FieldParams * len(params))(*params)
+    d = WorldDesc()
+    d.nx, d.ny, d.nz, d.n_fields = nx, ny, nz, len(params)
+    d.fields = C.cast(arr, C.POINTER(FieldParams))
+    d.pad_mode, d.epi_boundary = pad_mode, epi_boundary
+    for a in range(3):
+        d.fft[a] = int(fft[a])
+    d.method = int(method)
+    return d, arr
+
+
+def autotune(nx, ny, nz, params, pad_mode=PAD_ZERO, epi_boundary=0, fft=(0, 0, 0),
+             device=0, reps=3):
+    """Times every axis pass candidate for this shape on temporary worlds,
+    caches the fastest (later worlds of the shape use it) and returns one
+    dict per axis (x, y, z)."""
+    d, _arr = _world_desc(nx, ny, nz, params, pad_mode, epi_boundary, fft, METHOD_SEPARABLE)
+    out = (AxisTuning * 3)()
+    _check(lib().vfd_autotune(C.byref(d), device, int(reps), out))
+    return [out[a].as_dict() for a in range(3)]
+
+
+def autotune_set(nx, ny, nz, params, tuning, pad_mode=PAD_ZERO, epi_boundary=0,
+                 fft=(0, 0, 0), device=0):
+    """Pins a per-axis choice (dicts as autotune returns) for this shape."""
+    d, _arr = _world_desc(nx, ny, nz, params, pad_mode, epi_boundary, fft, METHOD_SEPARABLE)
+    inv = {v: k for k, v in PASS_METHODS.items()}
+    arr = (AxisTuning * 3)()
+    for a in range(3):
+        t = tuning[a]
+        m = t.get("method", "register_fft")
+        arr[a].method = inv.get(m, m)
+        arr[a].ctas_per_sm = int(t.get("ctas_per_sm", 0))
+        arr[a].fft_len = int(t.get("fft_len", 0))
+        arr[a].radix_order = int(t.get("radix_order", 0))
+        arr[a].variant = int(t.get("variant", -1))
+        arr[a].ms = float(t.get("ms", 0.0))
+    _check(lib().vfd_autotune_set(C.byref(d), device, arr))
+
+
+def autotune_clear():
+    _check(lib().vfd_autotune_clear())
+
+
 class World:
     """One world of `n_fields` fields on an nx*ny*nz grid (x fastest)."""
 
@@ -214,14 +273,7 @@ class World:
                  fft=(0, 0, 0), device=0, method=METHOD_SEPARABLE):
         self.nx, self.ny, self.nz = nx, ny, nz
         self.nf = len(params)
-        self._params = (FieldParams * self.nf)(*params)
-        d = WorldDesc()
-        d.nx, d.ny, d.nz, d.n_fields = nx, ny, nz, self.nf
-        d.fields = C.cast(self._params, C.POINTER(FieldParams))
-        d.pad_mode, d.epi_boundary = pad_mode, epi_boundary
-        for a in range(3):
-            d.fft[a] = int(fft[a])
-        d.method = int(method)
+        d, self._params = _world_desc(nx, ny, nz, params, pad_mode, epi_boundary, fft, method)
         h = C.c_void_p()
         _check(lib().vfd_world_create(C.byref(d), device, C.byref(h)))
         self._h = h
@@ -260,6 +312,12 @@ class World:
         b = C.c_size_t()
         _check(lib().vfd_world_device_bytes(self._h, C.byref(b)), self._h)
         return b.value
+
+    def tuning(self):
+        """The pass each axis runs, one dict per axis (x, y, z)."""
+        out = (AxisTuning * 3)()
+        _check(lib().vfd_world_tuning(self._h, out), self._h)
+        return [out[a].as_dict() for a in range(3)]
 
     def upload(self, field, arr, stream=None):
         a = np.ascontiguousarray(arr, dtype=np.float32)
