@@ -1,24 +1,34 @@
 // vfd_rf.cu -- one axis of the separable FFT convolution, overlap-save with
-// 64-point blocks, each block's FFT held by ONE thread in 64 complex
-// registers.
+// 64-point blocks, each block's FFT held by ONE thread in registers.
 //
 // Same method as vfd_os.cu (blocks of L = 64 - 2r outputs; forward FFT-64,
 // multiply by the kernel's 64-point spectrum, inverse FFT-64, keep L samples
 // -- the reference's pad / R2C / modulate / C2R / crop, Diffusion.cu:1731-1859,
-// per block; lines 2p and 2p+1 ride in one complex FFT).  What changes is who
-// holds a block: a thread owns a line pair and walks its blocks in order.
-// The FFT-64 is radix 8 x 8 entirely in registers: its transpose is register
-// renaming and its twiddles are constant-bank operands, so a block costs no
-// shared-memory traffic beyond its input and output.
+// per block; lines 2p and 2p+1 ride in one complex FFT as its real and
+// imaginary parts).  What changes is who holds a block: a thread owns a line
+// pair and walks its blocks in order.
 //
-//   y and z passes (lines contiguous in x): a warp owns 32 adjacent pairs
-//   (64 lines); at each position the warp loads and stores 256 contiguous
-//   bytes straight from and to global memory.
+// Register layout ("split pairs"): the 64 complex samples x[0..63] of a block
+// sit in 32 slots of two float2 registers, slot j = {re: (Re x[2j], Re x[2j+1]),
+// im: (Im x[2j], Im x[2j+1])}.  Lane .x of every slot is the even-sample
+// sequence, lane .y the odd one, so ONE packed FFT-32 (radix 8 x 4; every
+// add, subtract and twiddle multiply a packed FP32x2 instruction on both
+// sequences, the transposes register renaming, the twiddles constant-bank
+// pairs) transforms both.  The radix-2 step that joins them into the 64-point
+// spectrum, the spectrum multiply and the radix-2 step that splits it again
+// for the inverse are one 2x2 map per bin pair (k, k + 32) (s_middle); the
+// inverse FFT-32 then leaves outputs 2m, 2m+1 side by side in slot m.
+//
+//   y and z passes (lines contiguous in x): a warp owns a tile of 64
+//   adjacent lines, lane k the pair (k, k + 32); at each position the warp
+//   loads and stores two runs of 128 contiguous bytes straight from and to
+//   global memory.  A CTA of W warps takes W
+//   tiles of one job and meets at one barrier per block.
 //   x pass (positions contiguous): a warp owns 64 rows; each block's window
 //   is copied row by row with 16-byte cp.async into a shared tile, each
-//   thread reads its pair's two rows, and outputs go back the same way with
-//   16-byte stores (rows 16-byte aligned and n a multiple of 4; otherwise
-//   the x pass uses the overlap-save kernel).
+//   thread reads its pair's two rows (16-byte reads land whole slots), and
+//   outputs go back the same way with 16-byte stores (rows 16-byte aligned
+//   and n a multiple of 4; otherwise the x pass uses the overlap-save kernel).
 //
 // In place: block b's window starts r positions before its first output, so
 // it overlaps the previous block's last r outputs.  Those r outputs are held
@@ -41,12 +51,13 @@
 namespace vfd {
 
 __constant__ float2 c_rfw64[64];  // exp(-2 pi i m / 64), FP64-generated on the host
+// w = exp(-2 pi i m / 32) = wr + i wi as packed pairs: (wr, wr), (wi, wi), (-wi, -wi)
+__constant__ float2 c_spc[32], c_sps[32], c_spn[32];
 
 namespace {
 
 __device__ __forceinline__ float2 r_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 r_sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
-__device__ __forceinline__ float2 r_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
 
 __device__ __forceinline__ double r_warp_sum(double v)
 {
@@ -55,98 +66,167 @@ __device__ __forceinline__ double r_warp_sum(double v)
     return v;
 }
 
+// Two complex values side by side: lane .x and lane .y of re and im.
+struct sp2 {
+    float2 re, im;
+};
+
+__device__ __forceinline__ sp2 s_add(sp2 a, sp2 b) { return {r_add(a.re, b.re), r_add(a.im, b.im)}; }
+__device__ __forceinline__ sp2 s_sub(sp2 a, sp2 b) { return {r_sub(a.re, b.re), r_sub(a.im, b.im)}; }
+// a + (-i) b (forward) or a + i b (inverse); -i b = (b.im, -b.re)
 template <bool INV>
-__device__ __forceinline__ void r_dft4(float2 &a0, float2 &a1, float2 &a2, float2 &a3)
+__device__ __forceinline__ sp2 s_add_rot(sp2 a, sp2 b)
 {
-    const float2 t0 = r_add(a0, a2), t1 = r_sub(a0, a2);
-    const float2 t2 = r_add(a1, a3), d = r_sub(a1, a3);
-    a0 = r_add(t0, t2);
-    a2 = r_sub(t0, t2);
-    if (!INV) {  // t3 = -i d
-        a1 = make_float2(t1.x + d.y, t1.y - d.x);
-        a3 = make_float2(t1.x - d.y, t1.y + d.x);
-    } else {  // t3 = +i d
-        a1 = make_float2(t1.x - d.y, t1.y + d.x);
-        a3 = make_float2(t1.x + d.y, t1.y - d.x);
-    }
+    return INV ? sp2{r_sub(a.re, b.im), r_add(a.im, b.re)} : sp2{r_add(a.re, b.im), r_sub(a.im, b.re)};
+}
+// a - (-i) b (forward) or a - i b (inverse)
+template <bool INV>
+__device__ __forceinline__ sp2 s_sub_rot(sp2 a, sp2 b)
+{
+    return INV ? sp2{r_add(a.re, b.im), r_sub(a.im, b.re)} : sp2{r_sub(a.re, b.im), r_add(a.im, b.re)};
 }
 
-// DFT-8 of (v0 .. v7) in place, radix 2 x 4, w8 = exp(-+ i pi / 4).
+// DFT-4 in place: a_k <- sum_n a_n w4^(+-nk).
 template <bool INV>
-__device__ __forceinline__ void r_dft8(float2 &v0, float2 &v1, float2 &v2, float2 &v3, float2 &v4, float2 &v5,
-                                       float2 &v6, float2 &v7)
+__device__ __forceinline__ void s_dft4(sp2 &a0, sp2 &a1, sp2 &a2, sp2 &a3)
+{
+    const sp2 t0 = s_add(a0, a2), t1 = s_sub(a0, a2), t2 = s_add(a1, a3), d = s_sub(a1, a3);
+    a0 = s_add(t0, t2);
+    a2 = s_sub(t0, t2);
+    a1 = s_add_rot<INV>(t1, d);
+    a3 = s_sub_rot<INV>(t1, d);
+}
+
+// DFT-8 in place (v_k <- X_k), radix 2 x 4: X_k = E_k + w8^k O_k,
+// X_{k+4} = E_k - w8^k O_k with E, O the DFT-4 of the even and odd inputs.
+template <bool INV>
+__device__ __forceinline__ void s_dft8(sp2 &v0, sp2 &v1, sp2 &v2, sp2 &v3, sp2 &v4, sp2 &v5, sp2 &v6, sp2 &v7)
 {
     const float h = 0.707106781186547524400844362105f;
-    float2 e0 = v0, e1 = v2, e2 = v4, e3 = v6;
-    float2 o0 = v1, o1 = v3, o2 = v5, o3 = v7;
-    r_dft4<INV>(e0, e1, e2, e3);
-    r_dft4<INV>(o0, o1, o2, o3);
+    const float2 H = make_float2(h, h), NH = make_float2(-h, -h);
+    sp2 e0 = v0, e1 = v2, e2 = v4, e3 = v6, o0 = v1, o1 = v3, o2 = v5, o3 = v7;
+    s_dft4<INV>(e0, e1, e2, e3);
+    s_dft4<INV>(o0, o1, o2, o3);
+    v0 = s_add(e0, o0);
+    v4 = s_sub(e0, o0);
+    v2 = s_add_rot<INV>(e2, o2);
+    v6 = s_sub_rot<INV>(e2, o2);
     if (!INV) {
-        o1 = r_mul(make_float2(o1.x + o1.y, o1.y - o1.x), make_float2(h, h));
-        o3 = r_mul(make_float2(o3.y - o3.x, o3.x + o3.y), make_float2(h, -h));
-        v2 = make_float2(e2.x + o2.y, e2.y - o2.x);  // o2 * -i
-        v6 = make_float2(e2.x - o2.y, e2.y + o2.x);
+        // w8 z = h ((zr + zi) + i (zi - zr)); w8^3 z = h ((zi - zr) - i (zr + zi))
+        const float2 p = r_add(o1.re, o1.im), q = r_sub(o1.im, o1.re);
+        v1 = sp2{__ffma2_rn(p, H, e1.re), __ffma2_rn(q, H, e1.im)};
+        v5 = sp2{__ffma2_rn(p, NH, e1.re), __ffma2_rn(q, NH, e1.im)};
+        const float2 u = r_sub(o3.im, o3.re), s = r_add(o3.re, o3.im);
+        v3 = sp2{__ffma2_rn(u, H, e3.re), __ffma2_rn(s, NH, e3.im)};
+        v7 = sp2{__ffma2_rn(u, NH, e3.re), __ffma2_rn(s, H, e3.im)};
     } else {
-        o1 = r_mul(make_float2(o1.x - o1.y, o1.x + o1.y), make_float2(h, h));
-        o3 = r_mul(make_float2(o3.x + o3.y, o3.x - o3.y), make_float2(-h, h));
-        v2 = make_float2(e2.x - o2.y, e2.y + o2.x);  // o2 * +i
-        v6 = make_float2(e2.x + o2.y, e2.y - o2.x);
+        // conj(w8) z = h ((zr - zi) + i (zr + zi)); conj(w8^3) z = h (-(zr + zi) + i (zr - zi))
+        const float2 p = r_sub(o1.re, o1.im), q = r_add(o1.re, o1.im);
+        v1 = sp2{__ffma2_rn(p, H, e1.re), __ffma2_rn(q, H, e1.im)};
+        v5 = sp2{__ffma2_rn(p, NH, e1.re), __ffma2_rn(q, NH, e1.im)};
+        const float2 s = r_add(o3.re, o3.im), u = r_sub(o3.re, o3.im);
+        v3 = sp2{__ffma2_rn(s, NH, e3.re), __ffma2_rn(u, H, e3.im)};
+        v7 = sp2{__ffma2_rn(s, H, e3.re), __ffma2_rn(u, NH, e3.im)};
     }
-    v0 = r_add(e0, o0);
-    v4 = r_sub(e0, o0);
-    v1 = r_add(e1, o1);
-    v5 = r_sub(e1, o1);
-    v3 = r_add(e3, o3);
-    v7 = r_sub(e3, o3);
 }
 
-// Forward FFT-64 in registers.  In: x[n], n = 8 n1 + n2.  Out: bin
-// k = k1 + 8 k2 in slot 8 k1 + k2.
-//   DFT-8 over n1 for each n2 (slots n2 + 8 n1)  -> A(n2, k1) in slot 8 k1 + n2
-//   twiddle w64^(n2 k1)
-//   DFT-8 over n2 for each k1 (slots 8 k1 + n2)  -> X(k1 + 8 k2) in slot 8 k1 + k2
-__device__ __forceinline__ void r_fft64_fwd(float2 (&x)[64])
+// z * w32^m (forward) or z * conj(w32^m) (inverse), both lanes.
+template <bool INV>
+__device__ __forceinline__ sp2 s_tw(sp2 z, int m)
+{
+    const float2 c = c_spc[m], s = c_sps[m], n = c_spn[m];
+    if (!INV) return sp2{__ffma2_rn(z.re, c, __fmul2_rn(z.im, n)), __ffma2_rn(z.re, s, __fmul2_rn(z.im, c))};
+    return sp2{__ffma2_rn(z.re, c, __fmul2_rn(z.im, s)), __ffma2_rn(z.re, n, __fmul2_rn(z.im, c))};
+}
+
+// Packed FFT-32 of both lanes.  In: sample n = 4 n1 + n2 in slot n.  Out:
+// bin k = k1 + 8 k2 in slot 4 k1 + k2.
+//   DFT-8 over n1 for each n2        -> A(n2, k1) in slot 4 k1 + n2
+//   twiddle w32^(n2 k1)
+//   DFT-4 over n2 for each k1        -> X(k1 + 8 k2) in slot 4 k1 + k2
+__device__ __forceinline__ void s_fft32_fwd(sp2 (&P)[32])
 {
 #pragma unroll
-    for (int n2 = 0; n2 < 8; ++n2)
-        r_dft8<false>(x[n2], x[8 + n2], x[16 + n2], x[24 + n2], x[32 + n2], x[40 + n2], x[48 + n2], x[56 + n2]);
+    for (int n2 = 0; n2 < 4; ++n2)
+        s_dft8<false>(P[n2], P[4 + n2], P[8 + n2], P[12 + n2], P[16 + n2], P[20 + n2], P[24 + n2], P[28 + n2]);
 #pragma unroll
     for (int k1 = 1; k1 < 8; ++k1)
 #pragma unroll
-        for (int n2 = 1; n2 < 8; ++n2) x[8 * k1 + n2] = c_mul(x[8 * k1 + n2], c_rfw64[n2 * k1]);
+        for (int n2 = 1; n2 < 4; ++n2) P[4 * k1 + n2] = s_tw<false>(P[4 * k1 + n2], n2 * k1);
 #pragma unroll
-    for (int k1 = 0; k1 < 8; ++k1)
-        r_dft8<false>(x[8 * k1], x[8 * k1 + 1], x[8 * k1 + 2], x[8 * k1 + 3], x[8 * k1 + 4], x[8 * k1 + 5],
-                      x[8 * k1 + 6], x[8 * k1 + 7]);
+    for (int k1 = 0; k1 < 8; ++k1) s_dft4<false>(P[4 * k1], P[4 * k1 + 1], P[4 * k1 + 2], P[4 * k1 + 3]);
 }
 
-// Inverse of r_fft64_fwd (unnormalised): bins in its output order, x[n] out.
-__device__ __forceinline__ void r_fft64_inv(float2 (&x)[64])
+// Inverse of s_fft32_fwd (unnormalised): bins in its output slots, samples
+// back in natural slots.
+__device__ __forceinline__ void s_fft32_inv(sp2 (&P)[32])
 {
 #pragma unroll
-    for (int k1 = 0; k1 < 8; ++k1)
-        r_dft8<true>(x[8 * k1], x[8 * k1 + 1], x[8 * k1 + 2], x[8 * k1 + 3], x[8 * k1 + 4], x[8 * k1 + 5],
-                     x[8 * k1 + 6], x[8 * k1 + 7]);
+    for (int k1 = 0; k1 < 8; ++k1) s_dft4<true>(P[4 * k1], P[4 * k1 + 1], P[4 * k1 + 2], P[4 * k1 + 3]);
 #pragma unroll
     for (int k1 = 1; k1 < 8; ++k1)
 #pragma unroll
-        for (int n2 = 1; n2 < 8; ++n2) {
-            const float2 w = c_rfw64[n2 * k1];
-            x[8 * k1 + n2] = c_mul(x[8 * k1 + n2], make_float2(w.x, -w.y));
-        }
+        for (int n2 = 1; n2 < 4; ++n2) P[4 * k1 + n2] = s_tw<true>(P[4 * k1 + n2], n2 * k1);
 #pragma unroll
-    for (int n2 = 0; n2 < 8; ++n2)
-        r_dft8<true>(x[n2], x[8 + n2], x[16 + n2], x[24 + n2], x[32 + n2], x[40 + n2], x[48 + n2], x[56 + n2]);
+    for (int n2 = 0; n2 < 4; ++n2)
+        s_dft8<true>(P[n2], P[4 + n2], P[8 + n2], P[12 + n2], P[16 + n2], P[20 + n2], P[24 + n2], P[28 + n2]);
 }
 
-// Spectrum multiply: bin k sits in slot 8 (k mod 8) + k / 8.
-__device__ __forceinline__ void r_modulate(float2 (&x)[64], const float2 *hh)
+// Between the packed FFT-32s.  With E, O the 32-point spectra of the even and
+// odd samples (lanes .x, .y of bin k's slot), t = w64^k and H the kernel's
+// 64-point spectrum (1/64 folded in):
+//   X[k] = E + t O,  X[k+32] = E - t O            (radix-2 join)
+//   Y = H X                                        (spectrum multiply)
+//   E' = Y[k] + Y[k+32],  O' = (Y[k] - Y[k+32]) conj(t)   (radix-2 split)
+// i.e. E' = Hs E + Hd t O,  O' = Hs O + Hd conj(t) E  with Hs = H[k] + H[k+32],
+// Hd = H[k] - H[k+32].  Per bin k the table holds
+//   mt[2k] = (Hs, Hs, Hd C, Hd C),  mt[2k+1] = (Hd S, -Hd S, -Hd S, Hd S),
+// t = C - i S.  The inverse FFT-32 of E' gives outputs 2m, of O' outputs 2m+1.
+__device__ __forceinline__ void s_middle(sp2 (&P)[32], const float4 *mt)
 {
 #pragma unroll
-    for (int k = 0; k < 64; ++k) x[8 * (k & 7) + (k >> 3)] = r_mul(x[8 * (k & 7) + (k >> 3)], hh[k]);
+    for (int k = 0; k < 32; ++k) {
+        sp2 &q = P[4 * (k & 7) + (k >> 3)];
+        const float4 m0 = mt[2 * k], m1 = mt[2 * k + 1];
+        const float2 A = make_float2(m0.x, m0.y), B = make_float2(m0.z, m0.w);
+        const float2 D = make_float2(m1.x, m1.y), ND = make_float2(m1.z, m1.w);
+        const float2 sre = make_float2(q.re.y, q.re.x), sim = make_float2(q.im.y, q.im.x);
+        const float2 re = __ffma2_rn(sim, D, __ffma2_rn(sre, B, __fmul2_rn(q.re, A)));
+        const float2 im = __ffma2_rn(sre, ND, __ffma2_rn(sim, B, __fmul2_rn(q.im, A)));
+        q.re = re;
+        q.im = im;
+    }
 }
 
-}  // namespace
+// The middle table of a job from its spectrum HH (HH[k].x = H[k]) times
+// `scale`; threads t, t + nthreads, ... of the CTA each fill bins.
+__device__ __forceinline__ void s_fill_middle(float4 *mt, const float2 *HH, int t, int nthreads, float scale = 1.0f)
+{
+    for (int k = t; k < 32; k += nthreads) {
+        const float a = scale * HH[k].x, b = scale * HH[k + 32].x;
+        const float hs = a + b, hd = a - b;
+        const float2 w = c_rfw64[k];  // (C, -S)
+        const float dc = hd * w.x, ds = -hd * w.y;
+        mt[2 * k] = make_float4(hs, hs, dc, dc);
+        mt[2 * k + 1] = make_float4(ds, -ds, -ds, ds);
+    }
+}
+
+// Sample i of a block (lane i & 1 of slot i / 2) as (line a, line b).
+__device__ __forceinline__ float2 s_get(const sp2 (&P)[32], int i)
+{
+    return (i & 1) ? make_float2(P[i >> 1].re.y, P[i >> 1].im.y) : make_float2(P[i >> 1].re.x, P[i >> 1].im.x);
+}
+__device__ __forceinline__ void s_set(sp2 (&P)[32], int i, float2 v)
+{
+    if (i & 1) {
+        P[i >> 1].re.y = v.x;
+        P[i >> 1].im.y = v.y;
+    } else {
+        P[i >> 1].re.x = v.x;
+        P[i >> 1].im.x = v.y;
+    }
+}
 
 // ---------------------------------------------------------------------------
 // y / z passes: one warp = one tile of 64 lines (32 pairs) of one outer index.
@@ -156,246 +236,186 @@ __device__ __forceinline__ void rf_prefetch_l2(const void *p)
     asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
 }
 
-template <int R, bool V2>
-__device__ __forceinline__ void rf_col_body(const OsJob &J, const OsTileInfo &T, const float2 *hh,
-                                            float2 (*held)[32])
+template <int R, int W, bool ZL>
+__device__ __forceinline__ void rf_col_body(const OsJob &J, const OsTileInfo &T, int nreal, const float4 *mt,
+                                            float (*held)[64])
 {
     constexpr int L = 64 - 2 * R;
-    const int lane = threadIdx.x;
-    const int nreal = T.flags & 255;
-    const int line = 2 * lane;
-    const bool va = line < nreal, vb = line + 1 < nreal;
+    const int lane = threadIdx.x & 31;
+    const bool va = lane < nreal, vb = lane + 32 < nreal;
     const int n = J.n;
     const int64_t ps = J.pos_stride;
-    float *const base = J.data + T.outer * J.outer_stride + (int64_t)(T.l0 + line) * J.line_stride;
-    const bool zlast = J.kind == PASS_Z;
+    // line a = tile line `lane`, line b = tile line `lane + 32`: lines are
+    // adjacent (line stride 1), so b sits 128 bytes after a
+    constexpr int lb = 32;
+    float *const base = J.data + T.outer * J.outer_stride + (T.l0 + lane);
+    constexpr bool zlast = ZL;
     const float keep = J.keep, b = J.b;
     const int nblocks = (n + 2 * R + L - 1) / L;
-    // one output (or held-back output) of the pair at position o
-    auto put = [&](float *d, float2 v) {
-        if (V2) {
-            *reinterpret_cast<float2 *>(d) = v;
-        } else {
-            d[0] = v.x;
-            if (vb) d[1] = v.y;
-        }
+    // outputs of the pair at position pointer d
+    auto put = [&](float *d, float va_, float vb_) {
+        d[0] = va_;
+        if (vb) d[lb] = vb_;
     };
 
-    float2 lk = make_float2(0.0f, 0.0f), cv = lk, ot = lk;
-    if (va) {
-        for (int bi = 0; bi < nblocks; ++bi) {
+    float2 lk = make_float2(0.0f, 0.0f), ot = lk;
+    // W > 1: every warp of the CTA walks the same job, so all run nblocks
+    // iterations and meet at one barrier per block (warps of an SM
+    // sub-partition stay on the same instructions)
+    for (int bi = 0; bi < nblocks; ++bi) {
+        if (W > 1) __syncthreads();
+        if (va) {
             const int c = -R + bi * L;  // first output of the block
             const int p0 = c - R;       // first input
             const bool inner = p0 >= 0 && p0 + 64 <= n;  // window and outputs inside the line
             float *const w0 = base + (int64_t)p0 * ps;
-            float2 x[64];
+            sp2 P[32];
             {
                 const float *sp = w0;
                 if (inner) {
 #pragma unroll
-                    for (int i = 0; i < 64; ++i, sp += ps)
-                        x[i] = V2 ? *reinterpret_cast<const float2 *>(sp) : make_float2(sp[0], vb ? sp[1] : 0.0f);
-                } else if (V2) {
-#pragma unroll
-                    for (int i = 0; i < 64; ++i, sp += ps)
-                        x[i] = ((unsigned)(p0 + i) < (unsigned)n) ? *reinterpret_cast<const float2 *>(sp)
-                                                                  : make_float2(0.0f, 0.0f);
+                    for (int i = 0; i < 64; ++i, sp += ps) s_set(P, i, make_float2(sp[0], vb ? sp[lb] : 0.0f));
                 } else {
 #pragma unroll
                     for (int i = 0; i < 64; ++i, sp += ps) {
                         const bool in = (unsigned)(p0 + i) < (unsigned)n;
-                        x[i] = make_float2(in ? sp[0] : 0.0f, (in && vb) ? sp[1] : 0.0f);
+                        s_set(P, i, make_float2(in ? sp[0] : 0.0f, (in && vb) ? sp[lb] : 0.0f));
                     }
                 }
             }
-            // the next block's new samples start for L2 while this one is transformed
+            // the next block's new samples start for L2 while this one is
+            // transformed: lane k covers bytes 8k .. 8k + 7 of the tile's 256
             if (bi + 1 < nblocks) {
                 const int q0 = p0 + 64, q1 = min(p0 + L + 64, n);
-                const float *pp = base + (int64_t)q0 * ps;
-                for (int q = q0; q < q1; ++q, pp += ps) rf_prefetch_l2(pp);
+                const float *pp = base + lane + (int64_t)q0 * ps;  // tile line 2 lane
+                if (2 * lane < nreal)
+                    for (int q = q0; q < q1; ++q, pp += ps) rf_prefetch_l2(pp);
             }
             // the previous block's held-back outputs: positions p0 .. p0 + R - 1,
             // just loaded above as this window's first inputs
             if (bi > 0) {
 #pragma unroll
                 for (int i = 0; i < R; ++i)
-                    if ((unsigned)(p0 + i) < (unsigned)n) put(w0 + (int64_t)i * ps, held[i][lane]);
+                    if ((unsigned)(p0 + i) < (unsigned)n) put(w0 + (int64_t)i * ps, held[i][lane], held[i][32 + lane]);
             }
-            r_fft64_fwd(x);
-            r_modulate(x, hh);
-            r_fft64_inv(x);
-            float *d = w0 + (int64_t)R * ps;  // position of sample R = first output c
+            s_fft32_fwd(P);
+            s_middle(P, mt);
+            if (zlast) {
+                // + keep b on every output: on the DC bins of both inverse FFT-32s
+                // (keep itself is folded into the z pass's spectrum table)
+                const float2 kb = make_float2(keep * b, keep * b);
+                P[0].re = r_add(P[0].re, kb);
+                P[0].im = r_add(P[0].im, kb);
+            }
+            s_fft32_inv(P);
+            if (!inner) {
+                // outputs past the line ends within the kernel's reach: the leak
 #pragma unroll
-            for (int i = R; i < R + L; ++i, d += ps) {
-                const int o = c + i - R;
-                if (inner || (unsigned)o < (unsigned)n) {
-                    float2 v = x[i];
-                    if (zlast) {
-                        cv = r_add(cv, v);
-                        v = r_mul(r_add(v, make_float2(b, b)), make_float2(keep, keep));
-                        ot = r_add(ot, v);
+                for (int i = R; i < R + L; ++i) {
+                    const int o = c + i - R;
+                    if (!((unsigned)o < (unsigned)n) && o >= -R && o < n + R) lk = r_add(lk, s_get(P, i));
+                }
+            }
+            if (zlast && inner) {
+                // FP32 total of the kept outputs (lane .x: sample 2j, .y: 2j + 1)
+                float2 sa = make_float2(0.0f, 0.0f), sb = sa;
+#pragma unroll
+                for (int j = R / 2; j <= (R + L - 1) / 2; ++j) {
+                    const int i0 = 2 * j, i1 = 2 * j + 1;
+                    const bool k0 = i0 >= R && i0 < R + L, k1 = i1 >= R && i1 < R + L;
+                    const float2 ra = P[j].re, rb = P[j].im;
+                    sa = r_add(sa, make_float2(k0 ? ra.x : 0.0f, k1 ? ra.y : 0.0f));
+                    sb = r_add(sb, make_float2(k0 ? rb.x : 0.0f, k1 ? rb.y : 0.0f));
+                }
+                ot = r_add(ot, make_float2(sa.x + sa.y, sb.x + sb.y));
+            }
+            float *d = w0 + (int64_t)R * ps;  // position of sample R = first output c
+            if (inner) {
+#pragma unroll
+                for (int i = R; i < R + L; ++i, d += ps) {
+                    const float2 v = s_get(P, i);
+                    if (i >= L) {  // stored after the next block's loads
+                        held[i - L][lane] = v.x;
+                        held[i - L][32 + lane] = v.y;
+                    } else {
+                        put(d, v.x, v.y);
                     }
-                    if (i >= L) held[i - L][lane] = v;  // stored after the next block's loads
-                    else put(d, v);
-                } else if (o >= -R && o < n + R) {
-                    lk = r_add(lk, x[i]);
+                }
+            } else {
+#pragma unroll
+                for (int i = R; i < R + L; ++i, d += ps) {
+                    const int o = c + i - R;
+                    if ((unsigned)o < (unsigned)n) {
+                        const float2 v = s_get(P, i);
+                        if (zlast) ot = r_add(ot, v);
+                        if (i >= L) {
+                            held[i - L][lane] = v.x;
+                            held[i - L][32 + lane] = v.y;
+                        } else {
+                            put(d, v.x, v.y);
+                        }
+                    }
                 }
             }
         }
+    }
+    if (va) {
         // the last block's held-back outputs
         const int clast = -R + (nblocks - 1) * L;
 #pragma unroll
         for (int i = 0; i < R; ++i) {
             const int o = clast + L - R + i;
-            if ((unsigned)o < (unsigned)n) put(base + (int64_t)o * ps, held[i][lane]);
+            if ((unsigned)o < (unsigned)n) put(base + (int64_t)o * ps, held[i][lane], held[i][32 + lane]);
         }
     }
     double *mass = J.mass;
-    const double s_lk = r_warp_sum((double)(va ? lk.x : 0.0f) + (double)(vb ? lk.y : 0.0f));
-    if (J.kind == PASS_Y) {
+    double s_lk = r_warp_sum((double)(va ? lk.x : 0.0f) + (double)(vb ? lk.y : 0.0f));
+    if (!zlast) {
         if (lane == 0 && s_lk != 0.0) atomicAdd(mass + MS_LEAK_Y, s_lk);
     } else {
-        const double s_cv = r_warp_sum((double)(va ? cv.x : 0.0f) + (double)(vb ? cv.y : 0.0f));
+        // z outputs are keep (v + b): n kept and 2r leaked per line give back
+        // the convolution's kept total (cv) and leak
         const double s_ot = r_warp_sum((double)(va ? ot.x : 0.0f) + (double)(vb ? ot.y : 0.0f));
+        const double lines = (double)min(max(nreal, 0), 64);
+        const double s_cv = s_ot / (double)keep - (double)b * n * lines;
+        s_lk = s_lk / (double)keep - (double)b * (2 * R) * lines;
         if (lane == 0) {
             if (s_lk != 0.0) atomicAdd(mass + MS_LEAK_Z, s_lk);
             if (s_cv != 0.0) atomicAdd(mass + MS_CONV, s_cv);
             if (s_ot != 0.0) atomicAdd(mass + MS_OUT, s_ot);
         }
     }
-}
-
-// The same walk with the radius read from the job at run time: register
-// indices stay compile-time (every slot is tested against [r, r + L)), the
-// held-back outputs are indexed in shared memory.  One code body for every
-// radius keeps the kernel small enough for the instruction cache when warps
-// of different radii share an SM.
-template <bool V2>
-__device__ __forceinline__ void rf_col_body_rt(const OsJob &J, const OsTileInfo &T, const float2 *hh,
-                                               float2 (*held)[32])
-{
-    const int R = J.r, L = 64 - 2 * R;
-    const int lane = threadIdx.x;
-    const int nreal = T.flags & 255;
-    const int line = 2 * lane;
-    const bool va = line < nreal, vb = line + 1 < nreal;
-    const int n = J.n;
-    const int64_t ps = J.pos_stride;
-    float *const base = J.data + T.outer * J.outer_stride + (int64_t)(T.l0 + line) * J.line_stride;
-    const bool zlast = J.kind == PASS_Z;
-    const float keep = J.keep, b = J.b;
-    const int nblocks = (n + 2 * R + L - 1) / L;
-    auto put = [&](int o, float2 v) {
-        float *d = base + (int64_t)o * ps;
-        if (V2) {
-            *reinterpret_cast<float2 *>(d) = v;
-        } else {
-            d[0] = v.x;
-            if (vb) d[1] = v.y;
-        }
-    };
-
-    float2 lk = make_float2(0.0f, 0.0f), cv = lk, ot = lk;
-    if (va) {
-        for (int bi = 0; bi < nblocks; ++bi) {
-            const int c = -R + bi * L;
-            const int p0 = c - R;
-            float2 x[64];
-            {
-                const float *sp = base + (int64_t)p0 * ps;
-                if (V2) {
-#pragma unroll
-                    for (int i = 0; i < 64; ++i, sp += ps)
-                        x[i] = ((unsigned)(p0 + i) < (unsigned)n) ? *reinterpret_cast<const float2 *>(sp)
-                                                                  : make_float2(0.0f, 0.0f);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 64; ++i, sp += ps) {
-                        const bool in = (unsigned)(p0 + i) < (unsigned)n;
-                        x[i] = make_float2(in ? sp[0] : 0.0f, (in && vb) ? sp[1] : 0.0f);
-                    }
-                }
-            }
-            if (bi > 0)
-                for (int i = 0; i < R; ++i)
-                    if ((unsigned)(p0 + i) < (unsigned)n) put(p0 + i, held[i][lane]);
-            r_fft64_fwd(x);
-            r_modulate(x, hh);
-            r_fft64_inv(x);
-#pragma unroll
-            for (int i = 1; i < 63; ++i) {  // kept samples: i in [R, R + L), R in 1 .. 8
-                if (i < R || i >= R + L) continue;
-                const int o = c + i - R;
-                if ((unsigned)o < (unsigned)n) {
-                    float2 v = x[i];
-                    if (zlast) {
-                        cv = r_add(cv, v);
-                        v = r_mul(r_add(v, make_float2(b, b)), make_float2(keep, keep));
-                        ot = r_add(ot, v);
-                    }
-                    if (i >= L) held[i - L][lane] = v;  // stored after the next block's loads
-                    else put(o, v);
-                } else if (o >= -R && o < n + R) {
-                    lk = r_add(lk, x[i]);
-                }
-            }
-        }
-        const int clast = -R + (nblocks - 1) * L;
-        for (int i = 0; i < R; ++i) {
-            const int o = clast + L - R + i;
-            if ((unsigned)o < (unsigned)n) put(o, held[i][lane]);
-        }
-    }
-    double *mass = J.mass;
-    const double s_lk = r_warp_sum((double)(va ? lk.x : 0.0f) + (double)(vb ? lk.y : 0.0f));
-    if (J.kind == PASS_Y) {
-        if (lane == 0 && s_lk != 0.0) atomicAdd(mass + MS_LEAK_Y, s_lk);
-    } else {
-        const double s_cv = r_warp_sum((double)(va ? cv.x : 0.0f) + (double)(vb ? cv.y : 0.0f));
-        const double s_ot = r_warp_sum((double)(va ? ot.x : 0.0f) + (double)(vb ? ot.y : 0.0f));
-        if (lane == 0) {
-            if (s_lk != 0.0) atomicAdd(mass + MS_LEAK_Z, s_lk);
-            if (s_cv != 0.0) atomicAdd(mass + MS_CONV, s_cv);
-            if (s_ot != 0.0) atomicAdd(mass + MS_OUT, s_ot);
-        }
-    }
-}
-
-template <bool V2>
-__global__ void __launch_bounds__(32, 12) rf_col_rt_kernel(const OsJob *__restrict__ jobs,
-                                                           const OsTileInfo *__restrict__ tiles)
-{
-    __shared__ __align__(16) float2 hh[64];
-    __shared__ float2 held[RF_RMAX][32];
-    const OsTileInfo T = tiles[blockIdx.x];
-    const OsJob &J = jobs[T.job];
-    hh[threadIdx.x] = J.HH[threadIdx.x];
-    hh[threadIdx.x + 32] = J.HH[threadIdx.x + 32];
-    __syncwarp();
-    rf_col_body_rt<V2>(J, T, hh, held);
 }
 
 // One launch covers tiles of every radius: the CTA's job picks the variant.
-template <bool V2>
-__global__ void __launch_bounds__(32, 12) rf_col_kernel(const OsJob *__restrict__ jobs,
-                                                        const OsTileInfo *__restrict__ tiles)
+// A CTA of W warps takes W consecutive tiles, all of one job (the host pads
+// each job's tiles to a multiple of W with empty ones); a tile of another
+// job than the CTA's first is treated as empty, so every warp runs the same
+// number of blocks and barriers.
+// ZL: the z pass (decay, baseline and the output totals applied).
+template <int W, bool ZL>
+__global__ void __launch_bounds__(32 * W, 12 / W) rf_col_kernel(const OsJob *__restrict__ jobs,
+                                                                const OsTileInfo *__restrict__ tiles)
 {
-    __shared__ __align__(16) float2 hh[64];
-    __shared__ float2 held[RF_RMAX][32];  // held-back outputs [i][lane]
-    const OsTileInfo T = tiles[blockIdx.x];
-    const OsJob &J = jobs[T.job];
-    hh[threadIdx.x] = J.HH[threadIdx.x];
-    hh[threadIdx.x + 32] = J.HH[threadIdx.x + 32];
-    __syncwarp();
+    __shared__ __align__(16) float4 mt[64];
+    __shared__ float held[W][RF_RMAX][64];  // held-back outputs [warp][i][line]
+    const int warp = threadIdx.x >> 5;
+    const int job = tiles[(size_t)blockIdx.x * W].job;
+    const OsTileInfo T = tiles[(size_t)blockIdx.x * W + warp];
+    const int nreal = T.job == job ? (T.flags & 255) : 0;
+    const OsJob &J = jobs[job];
+    s_fill_middle(mt, J.HH, threadIdx.x, 32 * W, ZL ? J.keep : 1.0f);
+    if (W > 1) __syncthreads();
+    else __syncwarp();
     switch (J.r) {
-    case 1: rf_col_body<1, V2>(J, T, hh, held); break;
-    case 2: rf_col_body<2, V2>(J, T, hh, held); break;
-    case 3: rf_col_body<3, V2>(J, T, hh, held); break;
-    case 4: rf_col_body<4, V2>(J, T, hh, held); break;
-    case 5: rf_col_body<5, V2>(J, T, hh, held); break;
-    case 6: rf_col_body<6, V2>(J, T, hh, held); break;
-    case 7: rf_col_body<7, V2>(J, T, hh, held); break;
-    default: rf_col_body<8, V2>(J, T, hh, held); break;
+    case 1: rf_col_body<1, W, ZL>(J, T, nreal, mt, held[warp]); break;
+    case 2: rf_col_body<2, W, ZL>(J, T, nreal, mt, held[warp]); break;
+    case 3: rf_col_body<3, W, ZL>(J, T, nreal, mt, held[warp]); break;
+    case 4: rf_col_body<4, W, ZL>(J, T, nreal, mt, held[warp]); break;
+    case 5: rf_col_body<5, W, ZL>(J, T, nreal, mt, held[warp]); break;
+    case 6: rf_col_body<6, W, ZL>(J, T, nreal, mt, held[warp]); break;
+    case 7: rf_col_body<7, W, ZL>(J, T, nreal, mt, held[warp]); break;
+    default: rf_col_body<8, W, ZL>(J, T, nreal, mt, held[warp]); break;
     }
 }
 
@@ -404,8 +424,11 @@ __global__ void __launch_bounds__(32, 12) rf_col_kernel(const OsJob *__restrict_
 // so blocks are moved through a shared tile with 16-byte copies:
 //   * chunks start on multiples of 4: the first output is -Rh (Rh = r
 //     rounded up to 4) and blocks keep L4 outputs (L4 = L rounded down to a
-//     multiple of 4); a block's window is the 68 positions from c - Rh, and
-//     its FFT input starts e = Rh - r positions into it;
+//     multiple of 4); a block's window is the 68 positions from c - Rh;
+//   * the FFT input starts e = (Rh - r) & ~1 positions into the window (an
+//     even offset, so 16-byte reads of a row land whole slots), which puts
+//     the first output in sample R2 = Rh - e (r or r + 1; L4 <= L - 2 when
+//     r is odd keeps the last output at most 63 - r);
 //   * tile rows are 68 floats; line row 2q sits in tile row q and row 2q+1
 //     in tile row 32 + q, so a warp's 16-byte column reads (lane = pair) fall
 //     on distinct bank quads (68 floats = 272 bytes = 16 mod 128);
@@ -425,15 +448,17 @@ __device__ __forceinline__ void rf_cp16(float *smem, const float *gmem, bool val
 __device__ __forceinline__ int rf_trow(int row) { return (row & 1) * 32 + (row >> 1); }
 
 template <int R>
-__device__ __forceinline__ void rf_row_body(const OsJob &J, const OsTileInfo &T, const float2 *hh, float *A,
+__device__ __forceinline__ void rf_row_body(const OsJob &J, const OsTileInfo &T, const float4 *mt, float *A,
                                             float *held)
 {
     constexpr int L = 64 - 2 * R;
     constexpr int L4 = L & ~3;          // outputs kept per block
     constexpr int RH = (R + 3) & ~3;    // held-back outputs per block (multiple of 4)
-    constexpr int E = RH - R;           // FFT input offset in the window
+    constexpr int E = (RH - R) & ~1;    // FFT input offset in the window (even)
+    constexpr int R2 = RH - E;          // sample of the first output (even)
     constexpr int NST = (L4 - RH) / 4;  // chunks stored at once per row
     constexpr int NHD = RH / 4;         // held chunks per row
+    static_assert(R2 % 2 == 0 && R2 >= R && R2 + L4 - 1 + R <= 63, "x-pass block geometry");
     const int lane = threadIdx.x;
     const int nreal = T.flags & 255;
     const int n = J.n;
@@ -457,6 +482,9 @@ __device__ __forceinline__ void rf_row_body(const OsJob &J, const OsTileInfo &T,
         }
     }
     const int nblocks = (n + R + RH + L4 - 1) / L4;
+    const int hw = lane >> 4, cq = lane & 15;  // half-warp, 16-byte chunk
+    float *const rowp = base + (int64_t)hw * ls;  // row hw of the tile
+    static_assert(NST <= 16, "one chunk per lane of a half-warp");
     // stores the held-back outputs (positions pa .. pa + RH - 1) of every row
     auto put_held = [&](int pa) {
         for (int k = lane; k < nreal * NHD; k += 32) {
@@ -473,19 +501,21 @@ __device__ __forceinline__ void rf_row_body(const OsJob &J, const OsTileInfo &T,
     for (int bi = 0; bi < nblocks; ++bi) {
         const int c = -RH + bi * L4;  // first output, a multiple of 4
         const int pa = c - RH;        // window start, a multiple of 4
-        // ---- window [pa, pa + 68) of every row, 16-byte chunks ---------------
+        // ---- window [pa, pa + 64 + e) of every row, 16-byte chunks -----------
+        // half-warp h copies chunk `cq` of rows h, h + 2, ...: row 2t + h lands
+        // in tile row 32 h + t (a chunk lies wholly inside or outside the line)
         {
-            int row = lane / 17, cc = lane - 17 * (lane / 17);
-            for (int k = lane; k < nreal * 17; k += 32) {
-                const int p = pa + 4 * cc;
-                const bool v = (unsigned)p < (unsigned)n;  // a chunk lies wholly inside or outside
-                const float *src = base + (int64_t)row * ls;
-                rf_cp16(A + rf_trow(row) * RF_TS + 4 * cc, v ? src + p : src, v);
-                cc += 15;
-                row += 1;
-                if (cc >= 17) {
-                    cc -= 17;
-                    row += 1;
+            const int p = pa + 4 * cq;
+            const bool v = (unsigned)p < (unsigned)n;
+            const float *src = rowp + (v ? p : 0);
+            float *dst = A + (32 * hw) * RF_TS + 4 * cq;
+            for (int r = hw; r < nreal; r += 2, src += 2 * ls, dst += RF_TS) rf_cp16(dst, src, v);
+            if (E > 0) {  // chunk 16: positions pa + 64 .. pa + 67
+                const int p16 = pa + 64;
+                const bool v16 = (unsigned)p16 < (unsigned)n;
+                for (int r = lane; r < nreal; r += 32) {
+                    const float *s16 = base + (int64_t)r * ls;
+                    rf_cp16(A + rf_trow(r) * RF_TS + 64, v16 ? s16 + p16 : s16, v16);
                 }
             }
         }
@@ -494,68 +524,78 @@ __device__ __forceinline__ void rf_row_body(const OsJob &J, const OsTileInfo &T,
         __syncwarp();
         // the previous block's held-back outputs are this window's first RH positions
         if (bi > 0) put_held(pa);
-        // ---- this lane's pair: FFT-64 in registers ------------------------------
-        float2 x[64];
+        // ---- this lane's pair: slots from 16-byte reads of its two rows ---------
+        sp2 P[32];
         {
             const float4 *ra = reinterpret_cast<const float4 *>(A + lane * RF_TS);
             const float4 *rb = reinterpret_cast<const float4 *>(A + (32 + lane) * RF_TS);
 #pragma unroll
             for (int m = 0; m < 17; ++m) {
+                const int j0 = (4 * m - E) / 2;  // slot of the chunk's first two positions
+                if (j0 + 1 < 0 || j0 >= 32) continue;
                 const float4 u = ra[m], w = rb[m];
-                const float ua[4] = {u.x, u.y, u.z, u.w}, wa[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int i = 4 * m + k - E;
-                    if (i >= 0 && i < 64) x[i] = make_float2(ua[k], wa[k]);
-                }
+                if (j0 >= 0) P[j0] = sp2{make_float2(u.x, u.y), make_float2(w.x, w.y)};
+                if (j0 + 1 < 32) P[j0 + 1] = sp2{make_float2(u.z, u.w), make_float2(w.z, w.w)};
             }
         }
-        __syncwarp();  // every lane has its column: the tile is free for outputs
+        __syncwarp();  // every lane has its columns: the tile is free for outputs
         if (!vb) {
             // tile rows past the tile's lines hold stale data: zero the pair's missing line
 #pragma unroll
-            for (int i = 0; i < 64; ++i) x[i] = make_float2(va ? x[i].x : 0.0f, 0.0f);
+            for (int j = 0; j < 32; ++j) {
+                P[j].im = make_float2(0.0f, 0.0f);
+                if (!va) P[j].re = make_float2(0.0f, 0.0f);
+            }
         }
         if (masked) {
 #pragma unroll
             for (int i = 0; i < 64; ++i) {
-                const int p = c - R + i;
+                const int p = c - R2 + i;
                 const bool px = p >= xlo && p < xhi;
-                x[i].x = (in_a && px) ? x[i].x - b : 0.0f;
-                x[i].y = (in_b && px) ? x[i].y - b : 0.0f;
+                float2 v = s_get(P, i);
+                v.x = (in_a && px) ? v.x - b : 0.0f;
+                v.y = (in_b && px) ? v.y - b : 0.0f;
+                s_set(P, i, v);
             }
         }
         {
-            float2 s2 = make_float2(0.0f, 0.0f);  // input mass: block outputs' positions
+            // input mass: the block outputs' positions (slots R2 / 2 .. (R2 + L4) / 2)
+            float2 sa = make_float2(0.0f, 0.0f), sb = sa;
 #pragma unroll
-            for (int i = R; i < R + L4; ++i) s2 = r_add(s2, x[i]);
-            acc_in += (double)(va ? s2.x : 0.0f) + (double)(vb ? s2.y : 0.0f);
+            for (int j = R2 / 2; j < (R2 + L4) / 2; ++j) {
+                sa = r_add(sa, P[j].re);
+                sb = r_add(sb, P[j].im);
+            }
+            acc_in += (double)(va ? sa.x + sa.y : 0.0f) + (double)(vb ? sb.x + sb.y : 0.0f);
         }
-        r_fft64_fwd(x);
-        r_modulate(x, hh);
-        r_fft64_inv(x);
+        s_fft32_fwd(P);
+        s_middle(P, mt);
+        s_fft32_inv(P);
 #pragma unroll
-        for (int i = R; i < R + L4; ++i) {
-            const int o = c + i - R;
-            if (!((unsigned)o < (unsigned)n) && o >= -R && o < n + R) lk = r_add(lk, x[i]);
+        for (int i = R2; i < R2 + L4; ++i) {
+            const int o = c + i - R2;
+            if (!((unsigned)o < (unsigned)n) && o >= -R && o < n + R) lk = r_add(lk, s_get(P, i));
         }
         {
             float4 *wa = reinterpret_cast<float4 *>(A + lane * RF_TS);
             float4 *wb = reinterpret_cast<float4 *>(A + (32 + lane) * RF_TS);
 #pragma unroll
             for (int m = 0; m < L4 / 4; ++m) {
-                wa[m] = make_float4(x[R + 4 * m].x, x[R + 4 * m + 1].x, x[R + 4 * m + 2].x, x[R + 4 * m + 3].x);
-                wb[m] = make_float4(x[R + 4 * m].y, x[R + 4 * m + 1].y, x[R + 4 * m + 2].y, x[R + 4 * m + 3].y);
+                const int j = R2 / 2 + 2 * m;
+                wa[m] = make_float4(P[j].re.x, P[j].re.y, P[j + 1].re.x, P[j + 1].re.y);
+                wb[m] = make_float4(P[j].im.x, P[j].im.y, P[j + 1].im.x, P[j + 1].im.y);
             }
         }
         __syncwarp();
         // ---- outputs [c, c + L4 - RH) of every row; the rest is held back ------
-        for (int k = lane; k < nreal * NST; k += 32) {
-            const int row = k / NST, cc = k - row * NST;
-            const int o = c + 4 * cc;
-            if ((unsigned)o < (unsigned)n)
-                *reinterpret_cast<float4 *>(base + (int64_t)row * ls + o) =
-                    *reinterpret_cast<const float4 *>(A + rf_trow(row) * RF_TS + 4 * cc);
+        {
+            const int o = c + 4 * cq;
+            if (cq < NST && (unsigned)o < (unsigned)n) {
+                float *dst = rowp + o;
+                const float *src = A + (32 * hw) * RF_TS + 4 * cq;
+                for (int r = hw; r < nreal; r += 2, dst += 2 * ls, src += RF_TS)
+                    *reinterpret_cast<float4 *>(dst) = *reinterpret_cast<const float4 *>(src);
+            }
         }
         for (int k = lane; k < nreal * NHD; k += 32) {
             const int row = k / NHD, cc = k - row * NHD;
@@ -579,23 +619,24 @@ __global__ void __launch_bounds__(32, 12) rf_row_kernel(const OsJob *__restrict_
 {
     __shared__ __align__(16) float A[64 * RF_TS];
     __shared__ __align__(16) float held[64 * 8];  // held-back outputs [row][RH]
-    __shared__ __align__(16) float2 hh[64];
+    __shared__ __align__(16) float4 mt[64];
     const OsTileInfo T = tiles[blockIdx.x];
     const OsJob &J = jobs[T.job];
-    hh[threadIdx.x] = J.HH[threadIdx.x];
-    hh[threadIdx.x + 32] = J.HH[threadIdx.x + 32];
+    s_fill_middle(mt, J.HH, threadIdx.x, 32);
     __syncwarp();
     switch (J.r) {
-    case 1: rf_row_body<1>(J, T, hh, A, held); break;
-    case 2: rf_row_body<2>(J, T, hh, A, held); break;
-    case 3: rf_row_body<3>(J, T, hh, A, held); break;
-    case 4: rf_row_body<4>(J, T, hh, A, held); break;
-    case 5: rf_row_body<5>(J, T, hh, A, held); break;
-    case 6: rf_row_body<6>(J, T, hh, A, held); break;
-    case 7: rf_row_body<7>(J, T, hh, A, held); break;
-    default: rf_row_body<8>(J, T, hh, A, held); break;
+    case 1: rf_row_body<1>(J, T, mt, A, held); break;
+    case 2: rf_row_body<2>(J, T, mt, A, held); break;
+    case 3: rf_row_body<3>(J, T, mt, A, held); break;
+    case 4: rf_row_body<4>(J, T, mt, A, held); break;
+    case 5: rf_row_body<5>(J, T, mt, A, held); break;
+    case 6: rf_row_body<6>(J, T, mt, A, held); break;
+    case 7: rf_row_body<7>(J, T, mt, A, held); break;
+    default: rf_row_body<8>(J, T, mt, A, held); break;
     }
 }
+
+}  // namespace
 
 // ---------------------------------------------------------------------------
 static bool rf_row_enabled();
@@ -618,12 +659,7 @@ void rf_append_tiles(const OsJob &j, int job, std::vector<OsTileInfo> &out)
             ti.job = job;
             ti.outer = outer;
             ti.l0 = lt * RF_LINES;
-            const int nreal = std::min(RF_LINES, j.nlines - ti.l0);
-            // 8-byte pair accesses: every (pair, position) address even
-            const uintptr_t base = reinterpret_cast<uintptr_t>(j.data) +
-                                   sizeof(float) * (uintptr_t)(outer * j.outer_stride + (int64_t)ti.l0 * j.line_stride);
-            const bool v2 = j.kind != PASS_X && (base & 7) == 0 && (j.pos_stride & 1) == 0 && (nreal & 1) == 0;
-            ti.flags = nreal | (v2 ? 1 << 8 : 0);
+            ti.flags = std::min(RF_LINES, j.nlines - ti.l0);  // real lines
             out.push_back(ti);
         }
 }
@@ -639,16 +675,19 @@ static bool rf_row_enabled()
     return on == 1;
 }
 
-// VFD_RF_RT=1 selects the y/z kernel that reads the radius at run time (one
-// code body) instead of the one with a compiled variant per radius.
-static bool rf_col_runtime_radius()
+// Warps per CTA of the y/z kernel (VFD_RF_W: 1, 2, 4, 6 or 12; default 4:
+// on B200 the 512x256x384 world's y and z passes took 0.737 / 0.761 ms with
+// 4, 0.766 / 0.794 with 1, 0.768 / 0.775 with 12); the x kernel takes one
+// warp per CTA.
+int rf_cta_warps(int axis)
 {
-    static int on = -1;
-    if (on < 0) {
-        const char *e = getenv("VFD_RF_RT");
-        on = (e && e[0] == '1') ? 1 : 0;
+    static int w = -1;
+    if (w < 0) {
+        const char *e = getenv("VFD_RF_W");
+        const int v = e ? atoi(e) : 4;
+        w = (v == 1 || v == 2 || v == 4 || v == 6 || v == 12) ? v : 4;
     }
-    return on == 1;
+    return axis == PASS_X ? 1 : w;
 }
 
 static std::mutex g_rf_mu;
@@ -662,17 +701,27 @@ cudaError_t rf_prepare()
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lk(g_rf_mu);
     if (g_rf_done[dev]) return cudaSuccess;
-    float2 tw[64];
+    float2 tw[64], pc[32], ps[32], pn[32];
     for (int m = 0; m < 64; ++m) {
         const double a = 6.283185307179586476925286766559 * m / 64.0;
         tw[m] = make_float2((float)std::cos(a), (float)-std::sin(a));
     }
+    for (int m = 0; m < 32; ++m) {
+        const double a = 6.283185307179586476925286766559 * m / 32.0;
+        const float wr = (float)std::cos(a), wi = (float)-std::sin(a);
+        pc[m] = make_float2(wr, wr);
+        ps[m] = make_float2(wi, wi);
+        pn[m] = make_float2(-wi, -wi);
+    }
     e = cudaMemcpyToSymbol(c_rfw64, tw, sizeof(tw));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_spc, pc, sizeof(pc));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_sps, ps, sizeof(ps));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_spn, pn, sizeof(pn));
     if (e == cudaSuccess) g_rf_done[dev] = true;
     return e;
 }
 
-cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int axis, bool pairs8, cudaStream_t st)
+cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int axis, cudaStream_t st)
 {
     if (ntiles <= 0) return cudaSuccess;
     int dev = 0;
@@ -684,12 +733,36 @@ cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, in
         ready = dev >= 0 && dev < 64 && g_rf_done[dev];
     }
     if (!ready && (e = rf_prepare()) != cudaSuccess) return e;
-    if (axis == PASS_X) rf_row_kernel<<<ntiles, 32, 0, st>>>(jobs, tiles);
-    else if (rf_col_runtime_radius()) {
-        if (pairs8) rf_col_rt_kernel<true><<<ntiles, 32, 0, st>>>(jobs, tiles);
-        else rf_col_rt_kernel<false><<<ntiles, 32, 0, st>>>(jobs, tiles);
-    } else if (pairs8) rf_col_kernel<true><<<ntiles, 32, 0, st>>>(jobs, tiles);
-    else rf_col_kernel<false><<<ntiles, 32, 0, st>>>(jobs, tiles);
+    const int W = rf_cta_warps(axis);
+    if (ntiles % W != 0) return cudaErrorInvalidValue;
+    const int nb = ntiles / W;
+    if (axis == PASS_X) {
+        rf_row_kernel<<<ntiles, 32, 0, st>>>(jobs, tiles);
+    } else {
+        const bool z = axis == PASS_Z;
+        switch (W) {
+        case 2:
+            if (z) rf_col_kernel<2, true><<<nb, 64, 0, st>>>(jobs, tiles);
+            else rf_col_kernel<2, false><<<nb, 64, 0, st>>>(jobs, tiles);
+            break;
+        case 4:
+            if (z) rf_col_kernel<4, true><<<nb, 128, 0, st>>>(jobs, tiles);
+            else rf_col_kernel<4, false><<<nb, 128, 0, st>>>(jobs, tiles);
+            break;
+        case 6:
+            if (z) rf_col_kernel<6, true><<<nb, 192, 0, st>>>(jobs, tiles);
+            else rf_col_kernel<6, false><<<nb, 192, 0, st>>>(jobs, tiles);
+            break;
+        case 12:
+            if (z) rf_col_kernel<12, true><<<nb, 384, 0, st>>>(jobs, tiles);
+            else rf_col_kernel<12, false><<<nb, 384, 0, st>>>(jobs, tiles);
+            break;
+        default:
+            if (z) rf_col_kernel<1, true><<<nb, 32, 0, st>>>(jobs, tiles);
+            else rf_col_kernel<1, false><<<nb, 32, 0, st>>>(jobs, tiles);
+            break;
+        }
+    }
     note_launch();
     return cudaGetLastError();
 }

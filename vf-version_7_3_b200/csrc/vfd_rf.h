@@ -15,13 +15,16 @@ constexpr int RF_LINES = 64;  // lines per tile (32 line pairs, one warp)
 
 // Whether job j (its other fields set) can use the register-FFT pass.
 bool rf_eligible(const OsJob &j);
-// Appends the 64-line tiles of job `job` to `out` (flags: bits 0-7 real
-// lines, bit 8: pair loads of 8 bytes apply).
+// Appends the 64-line tiles of job `job` to `out` (flags: real lines).
 void rf_append_tiles(const OsJob &j, int job, std::vector<OsTileInfo> &out);
+// Warps per CTA of the pass along `axis`: a launch's tile list holds a
+// multiple of this many tiles, each CTA's tiles of one job (padded with
+// empty tiles, flags 0).
+int rf_cta_warps(int axis);
 // Uploads the FFT-64 twiddles to the current device (outside stream capture).
 cudaError_t rf_prepare();
 // One launch over `ntiles` tiles of jobs (any radius <= RF_RMAX) that all
-// belong to `axis`; pairs8: every tile allows 8-byte pair accesses (flag bit 8).
-cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int axis, bool pairs8, cudaStream_t st);
+// belong to `axis`.
+cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int axis, cudaStream_t st);
 
 }  // namespace vfd

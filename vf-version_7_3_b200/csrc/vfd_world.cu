@@ -202,7 +202,6 @@ using namespace vfd;
 // A register-FFT launch of one axis (tiles of every radius).
 struct RfGroup {
     int r = 0;  // unused: the kernel reads each tile's radius from its job
-    bool pairs8 = false;   // every tile allows 8-byte pair accesses
     int ntiles = 0;
     OsTileInfo *d_tiles = nullptr;
 };
@@ -228,11 +227,21 @@ static cudaError_t build_rf_groups(const OsJob *jobs, int n, std::vector<RfGroup
     // resident together on one compiled variant (instruction-cache locality)
     std::stable_sort(t.begin(), t.end(),
                      [&](const OsTileInfo &a, const OsTileInfo &b) { return jobs[a.job].r < jobs[b.job].r; });
+    // CTAs of W warps: each job's run of tiles padded to a multiple of W
+    const int W = rf_cta_warps(jobs[0].kind);
+    if (W > 1) {
+        std::vector<OsTileInfo> p;
+        p.reserve(t.size() + (size_t)n * W);
+        for (size_t i = 0; i < t.size(); ++i) {
+            p.push_back(t[i]);
+            if (i + 1 == t.size() || t[i + 1].job != t[i].job)
+                while (p.size() % W) p.push_back(OsTileInfo{t[i].job, 0, 0, 0});
+        }
+        t.swap(p);
+    }
     RfGroup g;
     g.r = 0;
     g.ntiles = (int)t.size();
-    g.pairs8 = true;
-    for (const auto &ti : t) g.pairs8 = g.pairs8 && ((ti.flags >> 8) & 1);
     cudaError_t e = cudaMalloc(&g.d_tiles, sizeof(OsTileInfo) * t.size());
     if (e == cudaSuccess) e = cudaMemcpy(g.d_tiles, t.data(), sizeof(OsTileInfo) * t.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
@@ -252,7 +261,7 @@ static void free_rf_groups(std::vector<RfGroup> &g)
 static cudaError_t launch_rf_groups(const OsJob *jobs, const std::vector<RfGroup> &g, int axis, cudaStream_t st)
 {
     for (const auto &x : g) {
-        cudaError_t e = launch_rf(jobs, x.d_tiles, x.ntiles, axis, x.pairs8, st);
+        cudaError_t e = launch_rf(jobs, x.d_tiles, x.ntiles, axis, st);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
