@@ -32,8 +32,8 @@ for p in (os.path.join(ROOT, "vf-version_7_3_b200"), ROOT):
 METRIC = "voxel-steps/s"
 # ncu dram__bytes_read.sum + dram__bytes_write.sum per y/z axis-pass launch of
 # this workload (8 fields of 512x256x384), scaled by voxels from the
-# 512x256x128 capture in profiles/rf_pass_512x256x128.md (3 x 1041 MB).
-AXIS_TRAFFIC_BYTES = 3.12e9
+# 512x256x128 capture in profiles/rf_pass_512x256x128.md (3 x 1038 MB).
+AXIS_TRAFFIC_BYTES = 3.11e9
 
 
 def peaks():

@@ -295,8 +295,19 @@ __global__ void __launch_bounds__(256) deposit_kernel(const DepositJob *__restri
         }
     }
     const int leader = __ffs(peers) - 1;
-    if (active && lane == leader) {
-        atomicAdd(jobs[j].data + vox, s);
+    const bool lead = active && lane == leader;
+    if (lead) atomicAdd(jobs[j].data + vox, s);
+    // FP64 source totals: one shared add per warp when the warp's sources
+    // belong to one field (the common case), else one per leader
+    const int j0 = __shfl_sync(0xffffffffu, j, 0);
+    if (__all_sync(0xffffffffu, !active || j == j0)) {
+        const double ws = warp_sum_d(lead ? (double)s : 0.0);
+        if (lane == 0 && ws != 0.0) {
+            const int slot = j0 - fbase;
+            if (slot >= 0 && slot < 8) atomicAdd(&fsum[slot], ws);
+            else atomicAdd(jobs[j0].mass + MS_SOURCES, ws);
+        }
+    } else if (lead) {
         const int slot = j - fbase;
         if (slot >= 0 && slot < 8) atomicAdd(&fsum[slot], (double)s);
         else atomicAdd(jobs[j].mass + MS_SOURCES, (double)s);
