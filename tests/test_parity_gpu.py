@@ -116,8 +116,7 @@ def test_constant_vf_padding_rule(gpu):
 
 
 # The pass a world uses depends on its shape and radii: the register-FFT pass
-# for radius <= 8 (y/z with 8-byte pair accesses when nx is even, 4-byte
-# otherwise; x with 16-byte tiles when nx is a multiple of 4, else the
+# for radius <= 8 (x with 16-byte tiles when nx is a multiple of 4, else the
 # overlap-save x pass), the overlap-save pass for radius 9..16.  Tiles of 64
 # lines end partly filled and with an odd line count on these grids.
 PATH_GRIDS = [(96, 70, 33), (70, 33, 41), (37, 65, 29), (132, 9, 66)]
@@ -136,6 +135,28 @@ def test_pass_paths_against_oracle(gpu, grid, sigmas):
         ref = oracle.tick(u, sigmas[f], dec[f], 2, idx, amt)
         assert rel_l2(outs[f], ref) <= REL_L2, (grid, sigmas[f])
         check_mass(outs[f], mass[f], 1 - dec[f], 0.0, nx * ny * nz)
+
+
+@pytest.mark.parametrize("sigmas", [[0.3, 0.6], [1.6, 2.0], [1.0, 2.3, 2.6]])
+def test_constant_vf_padding_every_x_block_offset(gpu, sigmas):
+    # radii 1, 2, 5, 6 start the x pass's FFT input 2 positions into its
+    # window, radii 3, 4, 7, 8 at the window start; the constant-VF rule is
+    # applied to the staged x samples in both cases
+    grid = (48, 40, 36)
+    nx, ny, nz = grid
+    dec = [0.02] * len(sigmas)
+    base = [3e-4 * (f + 1) for f in range(len(sigmas))]
+    inputs = []
+    for f in range(len(sigmas)):
+        u = vfd.synth_field(6, 1, f, (nz, ny, nx))
+        idx, amt = vfd.synth_sources(6, 1, f, 40, nx * ny * nz)
+        inputs.append((u, idx, amt))
+    outs, mass, _ = run_world(grid, sigmas, dec, inputs, substeps=2, pad_mode=vfd.PAD_CONSTANT_VF, epi=29,
+                              baselines=base)
+    for f, (u, idx, amt) in enumerate(inputs):
+        ref = oracle.tick(u, sigmas[f], dec[f], 2, idx, amt, b=float(np.float32(base[f])), pad_mode=1, epi=29)
+        assert rel_l2(outs[f], ref) <= REL_L2, sigmas[f]
+        check_mass(outs[f], mass[f], 1 - dec[f], float(np.float32(base[f])), nx * ny * nz)
 
 
 def test_constant_field_fixed_point(gpu):
