@@ -46,7 +46,7 @@ typedef enum vfd_status {
 } vfd_status;
 
 /* Boundary treatment of the padded FFT grid.
- * VFD_PAD_ZERO: the field is zero-extended (BASELINE configurations).
+ * VFD_PAD_ZERO: the field is zero-extended (the benchmark configurations).
  * VFD_PAD_CONSTANT_VF: the reference's padDataConstantVF3D rule
  *   (src/Diffusion/convolutionFFT.cuh:590-638): only 0<z<nz-1, 0<y<ny-1,
  *   0<x<epi_boundary keeps the field value; every other voxel of the FFT
