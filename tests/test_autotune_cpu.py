@@ -54,3 +54,4 @@ def test_general_methods_are_not_tuned():
     assert L.vfd_autotune_set(C.byref(d), 0, t) == 7  # VFD_ERR_NOT_SUPPORTED
     assert L.vfd_autotune_set(None, 0, t) == 1
     assert L.vfd_world_tuning(None, t) == 1
+
