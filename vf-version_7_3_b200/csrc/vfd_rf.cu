@@ -4,8 +4,9 @@
 // Same method as vfd_os.cu (blocks of L = 64 - 2r outputs; forward FFT-64,
 // multiply by the kernel's 64-point spectrum, inverse FFT-64, keep L samples
 // -- the reference's pad / R2C / modulate / C2R / crop, Diffusion.cu:1731-1859,
-// per block; lines 2p and 2p+1 ride in one complex FFT as its real and
-// imaginary parts).  What changes is who holds a block: a thread owns a line
+// per block; two lines ride in one complex FFT as its real and imaginary
+// parts: rows 2q and 2q+1 in the x pass, lines k and k+32 of a tile in the
+// y and z passes).  What changes is who holds a block: a thread owns a line
 // pair and walks its blocks in order.
 //
 // Register layout ("split pairs"): the 64 complex samples x[0..63] of a block
