@@ -86,3 +86,27 @@ def test_generator_matches_committed_fixture():
         np.testing.assert_array_equal(u.ravel()[:16], g["gen_u"][f])
         np.testing.assert_array_equal(idx[:16], g["gen_idx"][f])
         np.testing.assert_array_equal(amt[:16], g["gen_amt"][f])
+
+
+def test_header_is_plain_c(tmp_path):
+    # the boundary is a C ABI: the header compiles as strict C99 and every
+    # struct a binding mirrors has the size the ctypes mirror assumes
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "h.c"
+    src.write_text('#include "vfd.h"\n#include <stdio.h>\n'
+                   'int main(void) { printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(vfd_field_params), '
+                   'sizeof(vfd_world_desc), sizeof(vfd_mass), sizeof(vfd_axis_tuning), '
+                   'sizeof(vfd_request_desc), sizeof(vfd_request_info), sizeof(vfd_server_stats)); '
+                   'return 0; }\n')
+    exe = tmp_path / "h"
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                    "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    sizes = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True,
+                                            text=True).stdout.split()]
+    assert sizes == [C.sizeof(vfd.FieldParams), C.sizeof(vfd.WorldDesc), C.sizeof(vfd.Mass),
+                     C.sizeof(vfd.AxisTuning), C.sizeof(vfd.RequestDesc), C.sizeof(vfd.RequestInfo),
+                     C.sizeof(vfd.ServerStats)]
