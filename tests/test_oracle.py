@@ -200,3 +200,23 @@ def test_oracle_against_committed_cfg0_fixture():
         np.testing.assert_allclose(out.ravel()[g["sample_idx"]], g["sample"][f], rtol=1e-12, atol=1e-18)
         assert abs(out.sum() - g["sums"][f]) <= 1e-12 * abs(g["sums"][f])
         assert abs(np.sqrt((out ** 2).sum()) - g["l2"][f]) <= 1e-12 * g["l2"][f]
+
+
+@pytest.mark.parametrize("pad_mode", [0, 1])
+def test_cpu_port_matches_fp64_oracle(pad_mode):
+    # the FP32 OpenMP port timed as the CPU baseline computes the same step:
+    # relative L2 within 1e-5 of the FP64 oracle, deposit totals exact in FP64
+    nx, ny, nz = 37, 24, 19
+    rng = np.random.default_rng(3)
+    u = rng.uniform(0.0, 1e-3, (nz, ny, nx)).astype(np.float32)
+    idx = rng.integers(0, nx * ny * nz, 300).astype(np.int32)
+    amt = rng.lognormal(-6.0, 1.0, 300).astype(np.float32)
+    sig, rate, b, epi = (1.3, 0.8, 2.1), 0.04, (2e-4 if pad_mode else 0.0), 30
+    rad = tuple(oracle.radius_of(s) for s in sig)
+    ref = oracle.tick(u, sig, rate, 1, idx, amt, b=b, pad_mode=pad_mode, epi=epi)
+    got = u.copy()
+    oracle.port_substep(got, sig, rad, rate, b=b, pad_mode=pad_mode, epi=epi, nthreads=2)
+    total = oracle.port_deposit_total(got, idx, amt)
+    err = np.sqrt(((got.astype(np.float64) - ref) ** 2).sum() / (ref ** 2).sum())
+    assert err <= 1e-5, err
+    assert abs(total - got.astype(np.float64).sum()) <= 1e-9 * abs(total)  # FP64 total of the field
