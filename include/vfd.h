@@ -191,6 +191,42 @@ vfd_status vfd_set_sources(vfd_world *w, int field, const int32_t *idx,
 vfd_status vfd_set_window(vfd_world *w, int field, const float *window, int kw, int kh, int kd,
                           int cx, int cy, int cz);
 
+/* Reference-mode kernel given as its stored spectrum.  The reference keeps
+ * each chemical's kernel only as chem_cctx->h_kernelspectrum[ic]: the
+ * unscaled R2C transform of the wrapped window (padKernel3D) on the chemical
+ * FFT grid, FFTD x FFTH x (FFTW/2+1) complex values laid out [z][y][kx] as
+ * interleaved (re, im) floats, filled once by computeKernelSpectrum3D
+ * (Diffusion.cu:1540-1610) into a buffer allocated per chemical
+ * (DiffusionHelper.cpp:556-592).  kspec may be a host (pinned or pageable)
+ * or a device pointer; it is copied, so the caller may free it on return.
+ * (fx, fy, fz) must equal the world's FFT grid: create the world with
+ * desc.fft = {FFTW, FFTH, FFTD}.  The kernel sum K0 (used by the constant-VF
+ * rule) is Re kspec[0].  Worlds created with VFD_METHOD_FFT3D or
+ * VFD_METHOD_PLAIN only (VFD_ERR_NOT_SUPPORTED otherwise). */
+vfd_status vfd_set_spectrum(vfd_world *w, int field, const float *kspec, int fx, int fy, int fz);
+
+/* Changes the constant-VF padding of a VFD_METHOD_FFT3D / VFD_METHOD_PLAIN
+ * world between ticks: the x bound (the reference passes rightWallIndex =
+ * bmcx - 1 to every diffuseChemGPU call, woundHealingWorld.cpp:2407) and,
+ * when baselines is not NULL, each field's baseline (pbaseline[ic],
+ * woundHealingWorld.cpp:970-975).  VFD_ERR_NOT_SUPPORTED for separable
+ * worlds, whose passes carry the padding box in their job records. */
+vfd_status vfd_set_boundary(vfd_world *w, int epi_boundary, const float *baselines);
+
+/* Reference-mode tick epilogue on the device (WHChemical::update,
+ * WHChemical.cpp:420-450): one tick of n_substeps substeps in which the last
+ * substep's output t becomes
+ *     p = d + decay[f] * t,    d = 0,    total[f] = sum(p) (FP64)
+ * for every field f (the reference's pChem = dChem + tChem*cytokineDecay[ic],
+ * dChem = 0; its decay table is woundHealingWorld.cpp:2640-2648).  dchem
+ * holds n_fields device pointers of V floats (an entry, or dchem itself, may
+ * be NULL: d = 0).  In VFD_METHOD_FFT3D / VFD_METHOD_PLAIN worlds the update
+ * is fused into the crop store of the inverse x transform; separable worlds
+ * run it as one extra pass over the fields.  Registered sources
+ * (vfd_set_sources) are deposited after the update.  vfd_read_mass then
+ * reports total = sum(p) + sources.  Asynchronous on `stream`. */
+vfd_status vfd_tick_update(vfd_world *w, int n_substeps, float *const *dchem, const float *decay, void *stream);
+
 /* Reference-mode window itself (computeKernel3D, Diffusion.cu:1078-1531):
  * the 7-point stencil (centre 1 - 6 lambda - gamma_dt, six arms lambda)
  * applied n_steps times to a unit impulse; out receives the centred window
@@ -218,6 +254,15 @@ vfd_status vfd_read_mass(vfd_world *w, vfd_mass *out, void *stream);
  * Synchronous: returns when host_out holds the result. */
 vfd_status vfd_diffuse_host(vfd_world *w, const float *const *host_in,
                             float *const *host_out, int n_substeps);
+
+/* ---- drop-in of diffuseChemGPU followed by WHChemical::update
+ * (WHChemical.cpp:420-450) with the update on the device: for every field,
+ * host_p[f] (pChem) and host_d[f] (dChem) -> device, one tick whose last
+ * substep's crop stores p = d + decay[f] * t (vfd_tick_update), p -> host_p[f];
+ * host_d[f] is zeroed.  host_d (or an entry) may be NULL: d = 0.  FP64 totals
+ * through vfd_read_mass.  Synchronous. */
+vfd_status vfd_diffuse_update_host(vfd_world *w, float *const *host_p, float *const *host_d,
+                                   const float *decay, int n_substeps);
 
 /* ---- batched ensembles (sensitivity-analysis ensembles of many worlds) --
  * A batch references (does not own) n_worlds worlds on one device; they

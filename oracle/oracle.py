@@ -35,6 +35,7 @@ def lib():
         L.vfo_prepare.argtypes = [C.c_int, C.c_int, C.c_int, _P, C.c_double, C.c_int, C.c_int, _P]
         L.vfo_conv_sep_direct.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P, C.c_int, _P, C.c_int,
                                           _P, C.c_int, _P]
+        L.vfo_conv_sep_direct_mt.argtypes = L.vfo_conv_sep_direct.argtypes
         L.vfo_conv_fft3d.argtypes = [C.c_int] * 6 + [_P, _P, _P, _P, _P] + [C.c_int] * 6 + [_P]
         L.vfo_conv_fft3d.restype = C.c_int
         L.vfo_conv_direct3d.argtypes = [C.c_int] * 3 + [_P, _P, _P] + [C.c_int] * 6
@@ -128,6 +129,23 @@ def _substep64(u64, sigma3, rate, radius3=None, b=0.0, pad_mode=0, epi=0):
     lk = np.zeros(3, np.float64)
     lib().vfo_conv_sep_direct(nx, ny, nz, _p(v), _p(tx), r[0], _p(ty), r[1], _p(tz), r[2], _p(lk))
     return (1.0 - rate) * (b + v)
+
+
+def tick_mt(u, sigma3, rate, n_substeps, idx, amt, radius3=None):
+    """oracle.tick with the separable direct sums spread over OpenMP threads
+    (vfo_conv_sep_direct_mt): FP64 throughout, zero padding; for the
+    full-size grids.  Returns (out float64, leaked [x, y, z] of the last substep)."""
+    nz, ny, nx = np.shape(u)
+    s = [float(sigma3)] * 3 if np.isscalar(sigma3) else [float(v) for v in sigma3]
+    r = [radius_of(v) for v in s] if radius3 is None else (
+        [int(radius3)] * 3 if np.isscalar(radius3) else [int(v) for v in radius3])
+    tx, ty, tz = gauss_taps(s[0], r[0]), gauss_taps(s[1], r[1]), gauss_taps(s[2], r[2])
+    v = np.array(u, np.float64, copy=True, order="C")
+    lk = np.zeros(3, np.float64)
+    for _ in range(n_substeps):
+        lib().vfo_conv_sep_direct_mt(nx, ny, nz, _p(v), _p(tx), r[0], _p(ty), r[1], _p(tz), r[2], _p(lk))
+        v *= (1.0 - rate)
+    return deposit(v, idx, amt), lk
 
 
 def deposit(u64, idx, amt):

@@ -100,6 +100,41 @@ done:
     return rc;
 }
 
+// computeKernelSpectrum3D (Diffusion.cu:1533-1619) replayed: the window
+// (kD*kH*kW, centre kZ,kY,kX) wrapped onto the fftD*fftH*fftW grid by the
+// reference's padKernel3D, transformed by cuFFT R2C, copied to h_spec
+// (fftD*fftH*(fftW/2+1) complex values, interleaved) -- the reference's
+// h_kernelspectrum[ic].
+extern "C" int ref_kernel_spectrum(const float *h_win, int kD, int kH, int kW, int kZ, int kY, int kX, int fftD,
+                                   int fftH, int fftW, float *h_spec)
+{
+    int rc = 0;
+    float *d_win = nullptr, *d_pk = nullptr;
+    float2 *d_ks = nullptr;
+    cufftHandle fwd = 0;
+    bool have_fwd = false;
+    const size_t fsz = (size_t)fftD * fftH * fftW;
+    const size_t ssz = (size_t)fftD * fftH * (fftW / 2 + 1);
+    const size_t wsz = (size_t)kD * kH * kW;
+    RR_CHECK(cudaMalloc(&d_win, wsz * sizeof(float)));
+    RR_CHECK(cudaMalloc(&d_pk, fsz * sizeof(float)));
+    RR_CHECK(cudaMalloc(&d_ks, ssz * sizeof(float2)));
+    RR_CHECK(cudaMemcpy(d_win, h_win, wsz * sizeof(float), cudaMemcpyHostToDevice));
+    RR_CUFFT(cufftPlan3d(&fwd, fftD, fftH, fftW, CUFFT_R2C));
+    have_fwd = true;
+    RR_CHECK(cudaMemset(d_pk, 0, fsz * sizeof(float)));
+    padKernel3D(d_pk, d_win, fftD, fftH, fftW, kD, kH, kW, kZ, kY, kX);
+    RR_CHECK(cudaGetLastError());
+    RR_CUFFT(cufftExecR2C(fwd, (cufftReal *)d_pk, (cufftComplex *)d_ks));
+    RR_CHECK(cudaMemcpy(h_spec, d_ks, ssz * sizeof(float2), cudaMemcpyDeviceToHost));
+done:
+    if (have_fwd) cufftDestroy(fwd);
+    cudaFree(d_win);
+    cudaFree(d_pk);
+    cudaFree(d_ks);
+    return rc;
+}
+
 // Times the reference's per-field diffusion on the device, window spectrum
 // prepared once.  ms[0]: the kernels + cuFFT of one fftDiffuse3D call
 // (memset, padDataConstantVF3D, R2C, modulateAndNormalize3D, C2R,

@@ -52,6 +52,10 @@ def test_create_rejects_bad_arguments_without_touching_a_device():
     assert L.vfd_world_create(C.byref(d), 0, C.byref(h)) == 1
     assert L.vfd_world_destroy(None) == 1
     assert L.vfd_tick(None, 1, None) == 1
+    assert L.vfd_set_spectrum(None, 0, None, 8, 8, 8) == 1
+    assert L.vfd_set_boundary(None, 0, None) == 1
+    assert L.vfd_tick_update(None, 1, None, None, None) == 1
+    assert L.vfd_diffuse_update_host(None, None, None, None, 1) == 1
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device path")

@@ -55,9 +55,10 @@ def test_batch_matches_single_worlds_and_oracle(gpu):
             errs.append((i, f, rel_l2(got, ref_single), rel_l2(got, ref), rel_l2(ref_single, ref)))
     for e in errs:
         assert e[2] <= 1e-6 and e[3] <= 1e-5 and e[4] <= 1e-5, errs
-        m = worlds[i].mass()
+    for w in worlds:
+        m = w.mass()
         for f in range(3):
-            s_ = worlds[i].download(f).astype(np.float64).sum()
+            s_ = w.download(f).astype(np.float64).sum()
             assert abs(m[f]["total"] - s_) <= 1e-6 * abs(s_)
     for w in worlds + singles:
         w.close()

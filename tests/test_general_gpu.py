@@ -159,3 +159,89 @@ def test_stencil_window_on_device(gpu, lam, n, R):
     ref = oracle.stencil_power(lam, 0.0, n, R)
     assert float(np.abs(got - ref).max()) <= 1e-6 * float(ref.max())
     assert abs(float(got.astype(np.float64).sum()) - float(ref.sum())) <= 1e-5
+
+
+def _wrapped_spectrum(win, centre, fft):
+    """R2C of the window wrapped onto the FFT grid with its centre at index 0
+    (padKernel3D + cufftExecR2C, the reference's h_kernelspectrum layout)."""
+    fx, fy, fz = fft
+    kd, kh, kw = win.shape
+    cz, cy, cx = centre
+    g = np.zeros((fz, fy, fx), np.float64)
+    for z in range(kd):
+        for y in range(kh):
+            for x in range(kw):
+                g[(z - cz) % fz, (y - cy) % fy, (x - cx) % fx] += win[z, y, x]
+    return np.fft.rfftn(g).astype(np.complex64)
+
+
+@pytest.mark.parametrize("method", [vfd.METHOD_FFT3D, vfd.METHOD_PLAIN])
+def test_stored_spectrum_and_boundary_change(gpu, method):
+    """vfd_set_spectrum (the reference's stored kernel spectrum) gives the same
+    result as the window it came from, against the FP64 oracle; vfd_set_boundary
+    then moves epiBoundary and the baseline between ticks."""
+    grid = (40, 36, 30)
+    nx, ny, nz = grid
+    R = 6
+    fft = (64, 56, 48)
+    win = oracle.stencil_power(0.1, 0.0, 12, R).astype(np.float32)
+    spec = _wrapped_spectrum(win, (R, R, R), fft)
+    u = vfd.synth_field(12, 0, 0, (nz, ny, nx))
+    params = [vfd.field_params(1.0, 0.0, radius=R, baseline=3e-4)]
+    with vfd.World(nx, ny, nz, params, pad_mode=1, epi_boundary=33, fft=fft, method=method) as w:
+        w.set_spectrum(0, spec)
+        for epi, base in ((33, 3e-4), (25, 6e-4)):
+            w.set_boundary(epi, [base])
+            w.upload(0, u)
+            w.tick(1)
+            got = w.download(0)
+            v = u.astype(np.float64) - np.float32(base)
+            mask = np.zeros_like(v, bool)
+            mask[1:nz - 1, 1:ny - 1, 1:epi] = True
+            v[~mask] = 0.0
+            w64 = win.astype(np.float64)
+            ref = oracle.conv_direct3d(v, w64, (R, R, R)) + np.float32(base) * float(spec[0, 0, 0].real)
+            assert rel_l2(got, ref) <= REL_L2, (epi, rel_l2(got, ref))
+        with pytest.raises(vfd.VfdError):
+            w.set_spectrum(0, spec[:, :-8, :])  # another grid
+
+
+def test_spectrum_and_boundary_rejected_for_separable(gpu):
+    with vfd.World(16, 16, 16, [vfd.field_params(1.0, 0.0)]) as w:
+        with pytest.raises(vfd.VfdError) as e:
+            w.set_boundary(10)
+        assert e.value.status == 7
+
+
+@pytest.mark.parametrize("method", [vfd.METHOD_SEPARABLE, vfd.METHOD_FFT3D, vfd.METHOD_PLAIN])
+def test_tick_update_against_oracle(gpu, method):
+    """vfd_tick_update: p = d + decay * t, d = 0 (WHChemical::update,
+    WHChemical.cpp:420-450) after the tick's substeps, for every method; the
+    FP64 total is the updated field's sum (plus the deposited sources)."""
+    import torch
+    grid = (48, 40, 24)
+    nx, ny, nz = grid
+    sig = [1.1, 0.8]
+    decay = [0.319, 0.9284]  # the reference's retention factors for TNF, IL8
+    ins = configs.field_inputs(0, 9, grid, 50, n_fields=2)
+    ds = [vfd.synth_field(13, 0, f, (nz, ny, nx), 0.0, 1e-4) for f in range(2)]
+    params = [vfd.field_params(s, 0.0) for s in sig]
+    dev_d = [torch.from_numpy(d.copy()).cuda() for d in ds]
+    with vfd.World(nx, ny, nz, params, method=method) as w:
+        for f, (u, idx, amt) in enumerate(ins):
+            w.upload(f, u)
+            w.set_sources(f, idx, amt)
+        w.tick_update(decay, [t.data_ptr() for t in dev_d], n_substeps=2)
+        torch.cuda.synchronize()
+        outs = [w.download(f) for f in range(2)]
+        mass = w.mass()
+    for f, (u, idx, amt) in enumerate(ins):
+        t = np.asarray(u, np.float64)
+        for _ in range(2):
+            t = oracle._substep64(t, sig[f], 0.0)
+        ref = ds[f].astype(np.float64) + decay[f] * t
+        ref = oracle.deposit(np.ascontiguousarray(ref), idx, amt)
+        assert rel_l2(outs[f], ref) <= REL_L2, (method, f, rel_l2(outs[f], ref))
+        assert float(dev_d[f].abs().max()) == 0.0
+        s = outs[f].astype(np.float64).sum()
+        assert abs(mass[f]["total"] - s) <= 1e-6 * s

@@ -220,3 +220,17 @@ def test_cpu_port_matches_fp64_oracle(pad_mode):
     err = np.sqrt(((got.astype(np.float64) - ref) ** 2).sum() / (ref ** 2).sum())
     assert err <= 1e-5, err
     assert abs(total - got.astype(np.float64).sum()) <= 1e-9 * abs(total)  # FP64 total of the field
+
+
+def test_multithreaded_oracle_equals_serial_oracle():
+    """oracle.tick_mt (the OpenMP, column-blocked separable sums used for the
+    full-size parity tests) gives the serial O2 oracle's result."""
+    rng = np.random.default_rng(3)
+    u = rng.random((23, 30, 141)).astype(np.float32)
+    idx = rng.integers(0, u.size, 50).astype(np.int32)
+    amt = rng.random(50).astype(np.float32)
+    for sig in [(1.3, 0.8, 2.1), 0.4, (6.0, 1.0, 5.5)]:
+        a = oracle.tick(u, sig, 0.05, 3, idx, amt)
+        b, lk = oracle.tick_mt(u, sig, 0.05, 3, idx, amt)
+        assert float(np.abs(a - b).max()) <= 1e-15 * float(np.abs(a).max())
+        assert lk.shape == (3,)

@@ -5,9 +5,11 @@ memory in its own arena or pool, or that must not cause the device-wide
 synchronisation of cudaMalloc / cudaFree inside a per-tick loop.  The test
 allocates the field and the kernel spectrum itself (here with torch) and
 checks, on two calls in a row, that the result equals the library's regular
-entry point (a VFD_METHOD_FFT3D world with the same window) within the
-tolerance of the other parity tests.  This file is collected last so that a
-run stopping at the first failure has run every other test before it.
+entry point (a VFD_METHOD_FFT3D world with the same window) and the FP64
+oracle's direct 3D convolution, within the tolerance of the other parity
+tests, on FFT grids with radix-8 and odd lengths.  This file is collected last
+so that a run stopping at the first failure has run every other test before
+it.
 """
 import ctypes as C
 
@@ -26,12 +28,29 @@ def rel_l2(a, b):
     return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
 
 
-@pytest.mark.parametrize("pad_mode", [vfd.PAD_ZERO, vfd.PAD_CONSTANT_VF])
-def test_noalloc_matches_regular_entry_point(gpu, pad_mode):
+def oracle_substep(u, win, R, pad_mode, base, epi, keep):
+    """keep * (b * sum(w) + conv(M (u - b))) in FP64 (zero padding: b = 0, M = 1)."""
+    nz, ny, nx = u.shape
+    b = np.float64(np.float32(base)) if pad_mode == vfd.PAD_CONSTANT_VF else 0.0
+    v = u.astype(np.float64) - b
+    if pad_mode == vfd.PAD_CONSTANT_VF:
+        mask = np.zeros_like(v, bool)
+        mask[1:nz - 1, 1:ny - 1, 1:min(epi, nx)] = True
+        v[~mask] = 0.0
+    w64 = win.astype(np.float64)
+    return keep * (oracle.conv_direct3d(v, w64, (R, R, R)) + b * w64.sum())
+
+
+@pytest.mark.parametrize("pad_mode,grid,fft", [
+    (vfd.PAD_ZERO, (40, 36, 30), (56, 48, 42)),          # even x, 7-smooth, >= n + R
+    (vfd.PAD_CONSTANT_VF, (40, 36, 30), (56, 48, 42)),
+    (vfd.PAD_CONSTANT_VF, (40, 36, 28), (64, 45, 35)),   # radix-8 x, odd y and z lengths
+])
+def test_noalloc_matches_regular_entry_point(gpu, pad_mode, grid, fft):
     import torch
-    nx, ny, nz = 40, 36, 30
+    nx, ny, nz = grid
     R = 6
-    fx, fy, fz = 56, 48, 42                 # even x, 7-smooth, >= n + R
+    fx, fy, fz = fft
     base, epi, keep = 3e-4, 33, 0.95
     win = oracle.stencil_power(0.1333, 0.0, 12, R).astype(np.float32)
     u = vfd.synth_field(21, 0, 0, (nz, ny, nx))
@@ -67,6 +86,11 @@ def test_noalloc_matches_regular_entry_point(gpu, pad_mode):
         outs.append(field.cpu().numpy().copy())
     assert rel_l2(outs[0], ref1) <= 1e-5
     assert rel_l2(outs[1], ref2) <= 1e-5
+    # and against the FP64 oracle, two substeps chained
+    o1 = oracle_substep(u, win, R, pad_mode, base, epi, keep)
+    o2 = oracle_substep(o1, win, R, pad_mode, base, epi, keep)
+    assert rel_l2(outs[0], o1) <= 1e-5
+    assert rel_l2(outs[1], o2) <= 1e-5
 
 
 def test_noalloc_rejects_sizes_beyond_the_static_scratch(gpu):

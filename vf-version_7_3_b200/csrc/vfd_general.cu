@@ -163,11 +163,20 @@ __global__ void __launch_bounds__(NL *TL, MINB) c2r_x_kernel(const GenRowPass p)
     if (row < p.nrows) {
         const int r1 = row % p.rows_per_plane, r2 = row / p.rows_per_plane;
         float *dst = p.rdst + (int64_t)r1 * p.r_s1 + (int64_t)r2 * p.r_s2;
+        // fused WHChemical::update: p = d + decay t, d = 0 (same row layout as the field)
+        float *drow = (p.fuse_update && p.dchem) ? p.dchem + (int64_t)r1 * p.r_s1 + (int64_t)r2 * p.r_s2 : nullptr;
         for (int x = pg; x < p.nstore; x += NPG) {
             float t = Sf[x * 2 * LS + sidx];
             if (p.fuse_crop) {
                 acc_conv += (double)t;
                 t = p.keep * (t + p.b * p.k0);
+                if (p.fuse_update) {
+                    t *= p.upd_scale;
+                    if (drow) {
+                        t += drow[x];
+                        drow[x] = 0.0f;
+                    }
+                }
                 acc_out += (double)t;
             }
             dst[x] = t;
@@ -252,8 +261,9 @@ __global__ void modulate_kernel(float2 *C, const float2 *K, int64_t n, float sca
 
 // u = keep * P[z][y][x] over the data region (unpadResult3D + the decay),
 // with FP64 sums of the cropped convolution and of the output.
+// With fuse_update: u = d + upd_scale * keep * P and d = 0 (WHChemical::update).
 __global__ void crop_kernel(float *u, const float *P, int nx, int ny, int nz, int Fx, int Fy, float keep,
-                            double *mass_conv, double *mass_out)
+                            double *mass_conv, double *mass_out, int fuse_update, float upd_scale, float *dchem)
 {
     __shared__ double red[8];
     const int64_t V = (int64_t)nx * ny * nz;
@@ -263,12 +273,37 @@ __global__ void crop_kernel(float *u, const float *P, int nx, int ny, int nz, in
         const int64_t r = i / nx;
         const int y = (int)(r % ny), z = (int)(r / ny);
         const float t = P[(int64_t)x + (int64_t)Fx * (y + (int64_t)Fy * z)];
-        const float o = keep * t;
+        float o = keep * t;
+        if (fuse_update) {
+            o *= upd_scale;
+            if (dchem) {
+                o += dchem[i];
+                dchem[i] = 0.0f;
+            }
+        }
         ac += (double)t;
         ao += (double)o;
         u[i] = o;
     }
     block_sum_atomic_g<256>(ac, mass_conv, red);
+    block_sum_atomic_g<256>(ao, mass_out, red);
+}
+
+// p = d + scale p, d = 0 (d may be NULL): WHChemical::update after a
+// separable tick; FP64 total of p.
+__global__ void update_kernel(float *p, float *d, float scale, int64_t n, double *mass_out)
+{
+    __shared__ double red[8];
+    double ao = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float o = scale * p[i];
+        if (d) {
+            o += d[i];
+            d[i] = 0.0f;
+        }
+        p[i] = o;
+        ao += (double)o;
+    }
     block_sum_atomic_g<256>(ao, mass_out, red);
 }
 
@@ -443,10 +478,18 @@ cudaError_t launch_modulate(float2 *C, const float2 *K, int64_t n, float scale, 
 }
 
 cudaError_t launch_crop(float *u, const float *P, int nx, int ny, int nz, int Fx, int Fy, float keep,
-                        double *mass_conv, double *mass_out, cudaStream_t st)
+                        double *mass_conv, double *mass_out, cudaStream_t st, int fuse_update, float upd_scale,
+                        float *dchem)
 {
     crop_kernel<<<grid_for((int64_t)nx * ny * nz), 256, 0, st>>>(u, P, nx, ny, nz, Fx, Fy, keep, mass_conv,
-                                                                  mass_out);
+                                                                  mass_out, fuse_update, upd_scale, dchem);
+    note_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_update(float *p, float *d, float scale, int64_t n, double *mass_out, cudaStream_t st)
+{
+    update_kernel<<<grid_for(n), 256, 0, st>>>(p, d, scale, n, mass_out);
     note_launch();
     return cudaGetLastError();
 }

@@ -27,9 +27,14 @@ struct GenRowPass {
     int fuse_pad;
     int box_lo[3], box_hi[3];
     float b;
-    // fused crop epilogue on store (C2R): out = keep * (t + b * k0)
+    // fused crop epilogue on store (C2R): out = keep * (t + b * k0); with
+    // fuse_update additionally out <- d + upd_scale * out and d <- 0 (the
+    // WHChemical::update epilogue; dchem NULL means d = 0)
     int fuse_crop;
     float keep, k0;
+    int fuse_update;
+    float upd_scale;
+    float *dchem;
     double *mass_in, *mass_leak, *mass_conv, *mass_out;  // may be NULL
 };
 
@@ -54,7 +59,10 @@ cudaError_t launch_pad(float *P, const float *u, int nx, int ny, int nz, int Fx,
                        const int *hi, float b, cudaStream_t st);
 cudaError_t launch_modulate(float2 *C, const float2 *K, int64_t n, float scale, cudaStream_t st);
 cudaError_t launch_crop(float *u, const float *P, int nx, int ny, int nz, int Fx, int Fy, float keep,
-                        double *mass_conv, double *mass_out, cudaStream_t st);
+                        double *mass_conv, double *mass_out, cudaStream_t st, int fuse_update = 0,
+                        float upd_scale = 1.0f, float *dchem = nullptr);
+// p = d + scale * p, d = 0 (d may be NULL), FP64 total of p added to mass_out.
+cudaError_t launch_update(float *p, float *d, float scale, int64_t n, double *mass_out, cudaStream_t st);
 cudaError_t launch_sum(const float *P, int64_t n, double *out, cudaStream_t st);
 cudaError_t launch_outer_spectrum(float2 *K, const float *sx, const float *sy, const float *sz, int Fx, int Fy,
                                   int Fz, cudaStream_t st);

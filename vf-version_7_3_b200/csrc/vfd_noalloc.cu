@@ -15,11 +15,18 @@
 // host-side stand-in), so the first call on each device looks the address up
 // with cudaGetSymbolAddress while that device is current and caches it.
 // That first call therefore performs set-up work; make it before any stream
-// capture.  Every call shares the same array and overwrites it: calls that
-// overlap on the GPU (other streams, other host threads, the same device)
-// race on it, so serialise them.  Nothing in the array has to start at zero:
-// every element a call reads was written earlier by the same call.
+// capture.  The cache is keyed by the device's current CUDA context (its
+// unique id): after cudaDeviceReset the library's module is loaded into a
+// new context, and the next call looks the address up again (that call, too,
+// belongs outside stream capture).  Every call shares the same array and
+// overwrites it: calls that overlap on the GPU (other streams, other host
+// threads, the same device) race on it, so serialise them.  Nothing in the
+// array has to start at zero: every element a call reads was written by the
+// same call, or -- the twiddle tables -- by an earlier call of the same FFT
+// lengths in the same context, which later calls reuse.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <mutex>
 
@@ -35,7 +42,36 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 static std::mutex g_noalloc_mu;
-static unsigned char *g_noalloc_ptr[kMaxDevices] = {};
+// per device: the scratch address, the context it belongs to, and the FFT
+// lengths (with nz, which places the tables) whose twiddles it holds
+struct NoAllocSlot {
+    unsigned char *ptr = nullptr;
+    unsigned long long ctx = 0;
+    int tw_key[4] = {0, 0, 0, 0};
+};
+static NoAllocSlot g_noalloc[kMaxDevices];
+
+// Unique id of the calling thread's current context (0 when unavailable).
+static unsigned long long current_context_id()
+{
+    static PFN_cuCtxGetCurrent_v4000 get_cur = nullptr;
+    static PFN_cuCtxGetId_v12000 get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) == cudaSuccess &&
+            qa == cudaDriverEntryPointSuccess)
+            get_cur = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(a);
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) == cudaSuccess &&
+            qb == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(b);
+    });
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (!get_cur || !get_id || get_cur(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 // Twiddles exp(-2 pi i m / F), FP64, stored FP32.
 __global__ void noalloc_twiddle_kernel(float2 *tw, int F)
@@ -76,17 +112,29 @@ extern "C" vfd_status vfd_fft_diffuse3d_noalloc(float *field, const float *kspec
     if (spec_bytes + tw_bytes[0] + tw_bytes[1] + tw_bytes[2] > kNoAllocScratchBytes)
         return VFD_ERR_INVALID_ARG;  // larger than the fixed 32 MiB scratch
 
+    // an error left pending by the caller's earlier launches is not this call's
+    (void)cudaGetLastError();
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return VFD_ERR_CUDA;
     unsigned char *base = nullptr;
+    bool need_tw = true;
+    const int tw_key[4] = {fx, fy, fz, nz};
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
+        NoAllocSlot &slot = g_noalloc[dev];
+        if (cudaSetDevice(dev) != cudaSuccess) return VFD_ERR_CUDA;  // the device's context, current on this thread
+        const unsigned long long ctx = current_context_id();
+        if (!slot.ptr || ctx == 0 || ctx != slot.ctx) {
             void *p = nullptr;
             if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return VFD_ERR_CUDA;
-            g_noalloc_ptr[dev] = static_cast<unsigned char *>(p);
+            slot.ptr = static_cast<unsigned char *>(p);
+            slot.ctx = ctx;
+            for (int i = 0; i < 4; ++i) slot.tw_key[i] = 0;
         }
-        base = g_noalloc_ptr[dev];
+        base = slot.ptr;
+        need_tw = !(slot.tw_key[0] == fx && slot.tw_key[1] == fy && slot.tw_key[2] == fz && slot.tw_key[3] == nz);
+        // later calls of these lengths reuse the tables this call writes
+        for (int i = 0; i < 4; ++i) slot.tw_key[i] = need_tw ? 0 : tw_key[i];
     }
     float2 *C = reinterpret_cast<float2 *>(base);
     float2 *tw[3];
@@ -95,11 +143,15 @@ extern "C" vfd_status vfd_fft_diffuse3d_noalloc(float *field, const float *kspec
     tw[2] = reinterpret_cast<float2 *>(base + spec_bytes + tw_bytes[0] + tw_bytes[1]);
 
     cudaStream_t st = (cudaStream_t)stream;
-    for (int a = 0; a < 3; ++a) {
-        noalloc_twiddle_kernel<<<(F[a] + 255) / 256, 256, 0, st>>>(tw[a], F[a]);
-        note_launch();
+    if (need_tw) {
+        for (int a = 0; a < 3; ++a) {
+            noalloc_twiddle_kernel<<<(F[a] + 255) / 256, 256, 0, st>>>(tw[a], F[a]);
+            note_launch();
+        }
+        if (cudaGetLastError() != cudaSuccess) return VFD_ERR_CUDA;
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        for (int i = 0; i < 4; ++i) g_noalloc[dev].tw_key[i] = tw_key[i];
     }
-    if (cudaGetLastError() != cudaSuccess) return VFD_ERR_CUDA;
 
     int lo[3], hi[3];
     if (pad_mode == VFD_PAD_CONSTANT_VF) {

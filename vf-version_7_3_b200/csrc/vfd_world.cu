@@ -333,6 +333,7 @@ struct vfd_world {
     float2 *d_C = nullptr;           // spectrum scratch
     float *d_P = nullptr;            // full real grid scratch (plain)
     std::vector<float> k0;           // K(0,0,0) = sum of the window, per field
+    float *d_upd = nullptr;          // vfd_diffuse_update_host: the fields' dChem on the device
 
     std::string err;
 };
@@ -379,6 +380,7 @@ static void release(vfd_world *w)
     cudaFree(w->d_kspec);
     cudaFree(w->d_C);
     cudaFree(w->d_P);
+    cudaFree(w->d_upd);
     for (auto &t : w->timed) {
         cudaEventDestroy(t.start);
         cudaEventDestroy(t.stop);
@@ -1060,6 +1062,43 @@ vfd_status vfd_set_window(vfd_world *w, int field, const float *window, int kw, 
     return VFD_OK;
 }
 
+vfd_status vfd_set_spectrum(vfd_world *w, int field, const float *kspec, int fx, int fy, int fz)
+{
+    if (!w) return VFD_ERR_INVALID_ARG;
+    if (w->method == VFD_METHOD_SEPARABLE)
+        return fail(w, VFD_ERR_NOT_SUPPORTED, "stored spectra need VFD_METHOD_FFT3D or VFD_METHOD_PLAIN");
+    if (field < 0 || field >= w->nf || !kspec) return fail(w, VFD_ERR_INVALID_ARG, "bad field or NULL spectrum");
+    if (fx != w->F[0] || fy != w->F[1] || fz != w->F[2])
+        return fail(w, VFD_ERR_INVALID_ARG,
+                    "spectrum grid " + std::to_string(fx) + "x" + std::to_string(fy) + "x" + std::to_string(fz) +
+                        " differs from the world's FFT grid " + std::to_string(w->F[0]) + "x" +
+                        std::to_string(w->F[1]) + "x" + std::to_string(w->F[2]) +
+                        " (create the world with desc.fft = {FFTW, FFTH, FFTD})");
+    DeviceGuard g(w->device);
+    const int64_t nk = (int64_t)w->Fxh * w->F[1] * w->F[2];
+    float2 *K = w->d_kspec + nk * field;
+    // cudaMemcpyDefault: host (pinned or pageable) or device source
+    VFD_CUDA(w, cudaMemcpy(K, kspec, sizeof(float2) * nk, cudaMemcpyDefault));
+    float2 dc;
+    VFD_CUDA(w, cudaMemcpy(&dc, K, sizeof(float2), cudaMemcpyDeviceToHost));
+    w->k0[field] = dc.x;
+    return VFD_OK;
+}
+
+vfd_status vfd_set_boundary(vfd_world *w, int epi_boundary, const float *baselines)
+{
+    if (!w) return VFD_ERR_INVALID_ARG;
+    if (w->method == VFD_METHOD_SEPARABLE)
+        return fail(w, VFD_ERR_NOT_SUPPORTED, "separable worlds fix their padding at creation");
+    if (baselines)
+        for (int f = 0; f < w->nf; ++f)
+            if (!std::isfinite(baselines[f])) return fail(w, VFD_ERR_INVALID_ARG, "baseline must be finite");
+    w->epi = epi_boundary;
+    if (baselines)
+        for (int f = 0; f < w->nf; ++f) w->params[f].baseline = baselines[f];
+    return VFD_OK;
+}
+
 // Uploads the concatenated source list and deposit jobs when they changed.
 static vfd_status sync_sources(vfd_world *w)
 {
@@ -1154,8 +1193,16 @@ struct LaunchTimer {
     }
 };
 
-// One substep of field f with the general 3D transform.
-static vfd_status enqueue_general_substep(vfd_world *w, int f, cudaStream_t st)
+// The WHChemical::update epilogue of vfd_tick_update: per field the device
+// array d (NULL: zero) and the retention factor of p = d + decay * t.
+struct UpdateArgs {
+    float *const *dchem;  // n_fields entries, or NULL
+    const float *decay;   // n_fields entries
+};
+
+// One substep of field f with the general 3D transform; with `upd` the crop
+// store applies the update epilogue.
+static vfd_status enqueue_general_substep(vfd_world *w, int f, cudaStream_t st, const UpdateArgs *upd = nullptr)
 {
     const int Fx = w->F[0], Fy = w->F[1], Fz = w->F[2];
     const int64_t nk = (int64_t)w->Fxh * Fy * Fz;
@@ -1221,6 +1268,11 @@ static vfd_status enqueue_general_substep(vfd_world *w, int f, cudaStream_t st)
         r.fuse_crop = 1;
         r.keep = keep;
         r.k0 = w->k0[f];
+        if (upd) {
+            r.fuse_update = 1;
+            r.upd_scale = upd->decay[f];
+            r.dchem = upd->dchem ? upd->dchem[f] : nullptr;
+        }
         r.mass_in = nullptr;
         r.mass_leak = mass + MS_LEAK_X;
         r.mass_conv = mass + MS_CONV;
@@ -1251,7 +1303,9 @@ static vfd_status enqueue_general_substep(vfd_world *w, int f, cudaStream_t st)
     VFD_CUDA(w, launch_gen_cols(w->gvar[1], col_pass(w, PASS_Y, w->d_C, Fz, Fy, Fy, GEN_INVERSE), st));
     VFD_CUDA(w, launch_gen_rows(w->gvar[0], r, true, st));
     VFD_CUDA(w, launch_sum(w->d_P, (int64_t)Fx * Fy * Fz, mass + MS_LEAK_X, st));  // full-grid sum, see read_mass
-    VFD_CUDA(w, launch_crop(u, w->d_P, w->nx, w->ny, w->nz, Fx, Fy, keep, mass + MS_CONV, mass + MS_OUT, st));
+    VFD_CUDA(w, launch_crop(u, w->d_P, w->nx, w->ny, w->nz, Fx, Fy, keep, mass + MS_CONV, mass + MS_OUT, st,
+                            upd ? 1 : 0, upd ? upd->decay[f] : 1.0f,
+                            (upd && upd->dchem) ? upd->dchem[f] : nullptr));
     return VFD_OK;
 }
 
@@ -1287,14 +1341,15 @@ static vfd_status enqueue_axis(vfd_world *w, int a, int field, cudaStream_t st)
     return VFD_OK;
 }
 
-static vfd_status enqueue_tick(vfd_world *w, int field, int n_substeps, cudaStream_t st)
+static vfd_status enqueue_tick(vfd_world *w, int field, int n_substeps, cudaStream_t st,
+                               const UpdateArgs *upd = nullptr)
 {
     if (w->method != VFD_METHOD_SEPARABLE) {
         const int f0 = field < 0 ? 0 : field, f1 = field < 0 ? w->nf : field + 1;
         for (int s = 0; s < n_substeps; ++s)
             for (int f = f0; f < f1; ++f) {
                 VFD_CUDA(w, cudaMemsetAsync(w->d_mass + (int64_t)f * MS_COUNT, 0, sizeof(double) * MS_COUNT, st));
-                vfd_status r = enqueue_general_substep(w, f, st);
+                vfd_status r = enqueue_general_substep(w, f, st, s + 1 == n_substeps ? upd : nullptr);
                 if (r != VFD_OK) return r;
             }
         if (field < 0) {
@@ -1317,6 +1372,17 @@ static vfd_status enqueue_tick(vfd_world *w, int field, int n_substeps, cudaStre
             vfd_status r = enqueue_axis(w, a, field, st);
             if (r != VFD_OK) return r;
             lt.done();
+        }
+    }
+    if (upd) {
+        // the update as one pass per field after the z pass (whose output
+        // total it replaces by the total of p)
+        const int f0 = field < 0 ? 0 : field, f1 = field < 0 ? w->nf : field + 1;
+        for (int f = f0; f < f1; ++f) {
+            double *m = w->d_mass + (int64_t)f * MS_COUNT + MS_OUT;
+            VFD_CUDA(w, cudaMemsetAsync(m, 0, sizeof(double), st));
+            VFD_CUDA(w, launch_update(w->d_fields + (int64_t)f * w->V, upd->dchem ? upd->dchem[f] : nullptr,
+                                      upd->decay[f], w->V, m, st));
         }
     }
     if (field < 0) {
@@ -1342,6 +1408,20 @@ vfd_status vfd_tick(vfd_world *w, int n_substeps, void *stream)
     vfd_status s = sync_sources(w);
     if (s != VFD_OK) return s;
     return enqueue_tick(w, -1, n_substeps, (cudaStream_t)stream);
+}
+
+vfd_status vfd_tick_update(vfd_world *w, int n_substeps, float *const *dchem, const float *decay, void *stream)
+{
+    if (!w) return VFD_ERR_INVALID_ARG;
+    if (n_substeps < 1) return fail(w, VFD_ERR_INVALID_ARG, "n_substeps must be >= 1");
+    if (!decay) return fail(w, VFD_ERR_INVALID_ARG, "decay is NULL");
+    for (int f = 0; f < w->nf; ++f)
+        if (!std::isfinite(decay[f])) return fail(w, VFD_ERR_INVALID_ARG, "decay must be finite");
+    DeviceGuard g(w->device);
+    vfd_status s = sync_sources(w);
+    if (s != VFD_OK) return s;
+    const UpdateArgs upd{dchem, decay};
+    return enqueue_tick(w, -1, n_substeps, (cudaStream_t)stream, &upd);
 }
 
 vfd_status vfd_read_mass(vfd_world *w, vfd_mass *out, void *stream)
@@ -1712,6 +1792,50 @@ vfd_status vfd_diffuse_host(vfd_world *w, const float *const *host_in, float *co
         VFD_CUDA(w, cudaStreamWaitEvent(w->s_out, w->ev_cmp[f], 0));
         VFD_CUDA(w, cudaMemcpyAsync(host_out[f], dev, bytes, cudaMemcpyDeviceToHost, w->s_out));
     }
+    VFD_CUDA(w, cudaStreamSynchronize(w->s_out));
+    VFD_CUDA(w, cudaStreamSynchronize(w->s_cmp));
+    int herr = 0;
+    VFD_CUDA(w, cudaMemcpy(&herr, w->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) return fail(w, VFD_ERR_DEVICE_FAULT, "a kernel rejected an out-of-range index");
+    return VFD_OK;
+}
+
+vfd_status vfd_diffuse_update_host(vfd_world *w, float *const *host_p, float *const *host_d, const float *decay,
+                                   int n_substeps)
+{
+    if (!w) return VFD_ERR_INVALID_ARG;
+    if (!host_p || !decay || n_substeps < 1)
+        return fail(w, VFD_ERR_INVALID_ARG, "NULL buffers, NULL decay or n_substeps < 1");
+    for (int f = 0; f < w->nf; ++f) {
+        if (!host_p[f]) return fail(w, VFD_ERR_INVALID_ARG, "NULL host buffer");
+        if (!std::isfinite(decay[f])) return fail(w, VFD_ERR_INVALID_ARG, "decay must be finite");
+    }
+    DeviceGuard g(w->device);
+    vfd_status s = sync_sources(w);
+    if (s != VFD_OK) return s;
+    const size_t bytes = sizeof(float) * w->V;
+    if (host_d && !w->d_upd) VFD_CUDA(w, cudaMalloc(&w->d_upd, bytes * w->nf));
+    std::vector<float *> dptr(w->nf, nullptr);
+    for (int f = 0; f < w->nf; ++f)
+        if (host_d && host_d[f]) dptr[f] = w->d_upd + (int64_t)f * w->V;
+    for (int f = 0; f < w->nf; ++f) {
+        float *dev = w->d_fields + (int64_t)f * w->V;
+        VFD_CUDA(w, cudaMemcpyAsync(dev, host_p[f], bytes, cudaMemcpyHostToDevice, w->s_in));
+        if (dptr[f]) VFD_CUDA(w, cudaMemcpyAsync(dptr[f], host_d[f], bytes, cudaMemcpyHostToDevice, w->s_in));
+        VFD_CUDA(w, cudaEventRecord(w->ev_in[f], w->s_in));
+        VFD_CUDA(w, cudaStreamWaitEvent(w->s_cmp, w->ev_in[f], 0));
+        // the update reads decay[f] and dchem[f] only for field f
+        const UpdateArgs upd{dptr.data(), decay};
+        s = enqueue_tick(w, f, n_substeps, w->s_cmp, &upd);
+        if (s != VFD_OK) return s;
+        VFD_CUDA(w, cudaEventRecord(w->ev_cmp[f], w->s_cmp));
+        VFD_CUDA(w, cudaStreamWaitEvent(w->s_out, w->ev_cmp[f], 0));
+        VFD_CUDA(w, cudaMemcpyAsync(host_p[f], dev, bytes, cudaMemcpyDeviceToHost, w->s_out));
+    }
+    // dChem = 0 on the host (WHChemical.cpp:427) once its copy has landed on the device
+    VFD_CUDA(w, cudaStreamSynchronize(w->s_in));
+    for (int f = 0; f < w->nf; ++f)
+        if (dptr[f]) std::memset(host_d[f], 0, bytes);
     VFD_CUDA(w, cudaStreamSynchronize(w->s_out));
     VFD_CUDA(w, cudaStreamSynchronize(w->s_cmp));
     int herr = 0;

@@ -45,6 +45,7 @@ EXPORTED = [
     "vfd_server_get_stats", "vfd_server_clock", "vfd_server_destroy",
     "vfd_fft_diffuse3d_noalloc", "vfd_update_gradients", "vfd_sample_field", "vfd_write_vtk",
     "vfd_autotune", "vfd_world_tuning", "vfd_autotune_set", "vfd_autotune_clear",
+    "vfd_set_spectrum", "vfd_set_boundary", "vfd_tick_update", "vfd_diffuse_update_host",
 ]
 
 PASS_METHODS = {0: "register_fft", 1: "overlap_save", 2: "full_line"}
@@ -136,6 +137,10 @@ def load(path=LIB_PATH):
     lib.vfd_world_set_profiling.argtypes = [P, C.c_int]
     lib.vfd_read_profile.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     lib.vfd_set_window.argtypes = [P, C.c_int, P] + [C.c_int] * 6
+    lib.vfd_set_spectrum.argtypes = [P, C.c_int, P, C.c_int, C.c_int, C.c_int]
+    lib.vfd_set_boundary.argtypes = [P, C.c_int, P]
+    lib.vfd_tick_update.argtypes = [P, C.c_int, C.POINTER(P), P, P]
+    lib.vfd_diffuse_update_host.argtypes = [P, C.POINTER(P), C.POINTER(P), P, C.c_int]
     lib.vfd_batch_create.argtypes = [C.POINTER(P), C.c_int, C.POINTER(P)]
     lib.vfd_batch_tick.argtypes = [P, C.c_int, P]
     lib.vfd_batch_destroy.argtypes = [P]
@@ -350,8 +355,41 @@ class World:
         cz, cy, cx = centre if centre is not None else (kd // 2, kh // 2, kw // 2)
         _check(lib().vfd_set_window(self._h, field, _ptr(w), kw, kh, kd, cx, cy, cz), self._h)
 
+    def set_spectrum(self, field, spec):
+        """Stored kernel spectrum, complex (Fz, Fy, Fx/2 + 1) on the world's FFT grid
+        (the reference's h_kernelspectrum[ic] layout)."""
+        a = np.ascontiguousarray(spec, dtype=np.complex64)
+        fz, fy, fxh = a.shape
+        fx = self.fft_dims()[0]
+        assert fxh == fx // 2 + 1
+        _check(lib().vfd_set_spectrum(self._h, field, _ptr(a), fx, fy, fz), self._h)
+
+    def set_boundary(self, epi_boundary, baselines=None):
+        b = None
+        if baselines is not None:
+            b = np.ascontiguousarray(baselines, dtype=np.float32)
+            assert b.size == self.nf
+        _check(lib().vfd_set_boundary(self._h, int(epi_boundary), None if b is None else _ptr(b)), self._h)
+
     def tick(self, n_substeps=1, stream=None):
         _check(lib().vfd_tick(self._h, n_substeps, stream), self._h)
+
+    def tick_update(self, decay, dchem_ptrs=None, n_substeps=1, stream=None):
+        """One tick whose last substep stores p = d + decay * t, d = 0 (device
+        pointers of the fields' dChem arrays, or None: d = 0)."""
+        dec = np.ascontiguousarray(decay, dtype=np.float32)
+        assert dec.size == self.nf
+        dp = None
+        if dchem_ptrs is not None:
+            dp = (C.c_void_p * self.nf)(*[p or None for p in dchem_ptrs])
+        _check(lib().vfd_tick_update(self._h, n_substeps, dp, _ptr(dec), stream), self._h)
+
+    def diffuse_update_host(self, host_p, host_d, decay, n_substeps=1):
+        """vfd_diffuse_update_host: host pChem in/out, host dChem in (zeroed)."""
+        dec = np.ascontiguousarray(decay, dtype=np.float32)
+        ps = (C.c_void_p * self.nf)(*[a.ctypes.data for a in host_p])
+        ds = None if host_d is None else (C.c_void_p * self.nf)(*[a.ctypes.data for a in host_d])
+        _check(lib().vfd_diffuse_update_host(self._h, ps, ds, _ptr(dec), n_substeps), self._h)
 
     def mass(self, stream=None):
         m = (Mass * self.nf)()
