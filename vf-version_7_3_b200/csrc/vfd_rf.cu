@@ -48,8 +48,13 @@
 #include "vfd_fft.cuh"
 #include "vfd_internal.h"
 #include "vfd_rf.h"
+#include "vfd_tma.h"
 
 namespace vfd {
+
+// Set when a pass's bounded wait for a bulk copy gave up (read and cleared by
+// rf_take_timeout).
+__device__ int g_rf_timeout = 0;
 
 __constant__ float2 c_rfw64[64];  // exp(-2 pi i m / 64), FP64-generated on the host
 // w = exp(-2 pi i m / 32) = wr + i wi as packed pairs: (wr, wr), (wi, wi), (-wi, -wi)
@@ -421,6 +426,195 @@ __global__ void __launch_bounds__(32 * W, 12 / W) rf_col_kernel(const OsJob *__r
 }
 
 // ---------------------------------------------------------------------------
+// y / z passes with TMA staging.  Same blocks, same FFT; what changes is how
+// a block's window reaches the registers: each warp owns a 64 x 64 float
+// window buffer in shared memory (positions x lines, 16 KB) and an mbarrier.
+// Lane 0 issues one 3D bulk tensor copy per window (the field seen as the
+// tensor {nx, ny, nz}; box {64 lines, 64 positions} along y or z); the
+// hardware fills positions outside the line with zeros, so loads need no
+// range tests.  Per block:
+//   wait for window b; every lane reads its pair's 64 samples (conflict-free
+//   4-byte reads: lane k reads columns k and k + 32); lane 0 issues the copy
+//   of window b + 1 into the same buffer; FFT, multiply, inverse FFT;
+//   outputs [c, c + L - r) go straight to global memory; the last r outputs
+//   -- positions that window b + 1 reads -- are stored once that copy has
+//   landed (it was in flight during the transform).
+// The waits are bounded (kTmaWaitCycles): a wait that gives up sets
+// g_rf_timeout and the warp stops.
+// ---------------------------------------------------------------------------
+template <int R, bool ZL>
+__device__ __forceinline__ void rf_col_tma_body(const OsJob &J, const CUtensorMap *map, const OsTileInfo &T,
+                                                int nreal, const float4 *mt, float *win, uint64_t *bar)
+{
+    constexpr int L = 64 - 2 * R;
+    const int lane = threadIdx.x & 31;
+    const bool va = lane < nreal, vb = lane + 32 < nreal;
+    const int n = J.n;
+    const int64_t ps = J.pos_stride;
+    constexpr int lb = 32;
+    float *const base = J.data + T.outer * J.outer_stride + (T.l0 + lane);
+    const float keep = J.keep, b = J.b;
+    const int nblocks = (n + 2 * R + L - 1) / L;
+    auto put = [&](float *d, float va_, float vb_) {
+        d[0] = va_;
+        if (vb) d[lb] = vb_;
+    };
+    // window of block bi: positions [-2R + bi L, -2R + bi L + 64) of lines [l0, l0 + 64)
+    auto issue = [&](int bi) {
+        const int p0 = -2 * R + bi * L;
+        mbar_arrive_expect_tx(bar, 64 * 64 * 4);
+        if (ZL) tma_load_3d(win, map, T.l0, T.outer, p0, bar);
+        else tma_load_3d(win, map, T.l0, p0, T.outer, bar);
+    };
+    if (lane == 0) issue(0);
+    float2 lk = make_float2(0.0f, 0.0f), ot = lk;
+    int issued = 0;  // last window issued
+    bool ok = true;
+    for (int bi = 0; bi < nblocks && ok; ++bi) {
+        // warp-uniform outcome: a lane whose wait gave up stops the whole warp
+        if (!__all_sync(0xffffffffu, mbar_wait(bar, bi & 1))) {
+            ok = false;
+            break;
+        }
+        const int c = -R + bi * L;  // first output of the block
+        const int p0 = c - R;       // first input
+        const bool inner = p0 >= 0 && p0 + 64 <= n;
+        sp2 P[32];
+#pragma unroll
+        for (int i = 0; i < 64; ++i) s_set(P, i, make_float2(win[i * 64 + lane], win[i * 64 + 32 + lane]));
+        __syncwarp();
+        const bool more = bi + 1 < nblocks;
+        if (more && lane == 0) {
+            fence_proxy_async_smem();  // the reads above before the copy overwrites the buffer
+            issue(bi + 1);
+        }
+        if (more) issued = bi + 1;
+        s_fft32_fwd(P);
+        s_middle(P, mt);
+        if (ZL) {
+            const float2 kb = make_float2(keep * b, keep * b);
+            P[0].re = r_add(P[0].re, kb);
+            P[0].im = r_add(P[0].im, kb);
+        }
+        s_fft32_inv(P);
+        if (!inner) {
+#pragma unroll
+            for (int i = R; i < R + L; ++i) {
+                const int o = c + i - R;
+                if (!((unsigned)o < (unsigned)n) && o >= -R && o < n + R) lk = r_add(lk, s_get(P, i));
+            }
+        }
+        if (ZL && inner) {
+            float2 sa = make_float2(0.0f, 0.0f), sb = sa;
+#pragma unroll
+            for (int j = R / 2; j <= (R + L - 1) / 2; ++j) {
+                const int i0 = 2 * j, i1 = 2 * j + 1;
+                const bool k0 = i0 >= R && i0 < R + L, k1 = i1 >= R && i1 < R + L;
+                const float2 ra = P[j].re, rb = P[j].im;
+                sa = r_add(sa, make_float2(k0 ? ra.x : 0.0f, k1 ? ra.y : 0.0f));
+                sb = r_add(sb, make_float2(k0 ? rb.x : 0.0f, k1 ? rb.y : 0.0f));
+            }
+            ot = r_add(ot, make_float2(sa.x + sa.y, sb.x + sb.y));
+        }
+        float *d = base + (int64_t)(p0 + R) * ps;  // position of sample R = first output c
+        // samples [R, L): positions no later window reads
+        if (va) {
+            if (inner) {
+#pragma unroll
+                for (int i = R; i < L; ++i, d += ps) {
+                    const float2 v = s_get(P, i);
+                    put(d, v.x, v.y);
+                }
+            } else {
+#pragma unroll
+                for (int i = R; i < L; ++i, d += ps) {
+                    const int o = c + i - R;
+                    if ((unsigned)o < (unsigned)n) {
+                        const float2 v = s_get(P, i);
+                        if (ZL) ot = r_add(ot, v);
+                        put(d, v.x, v.y);
+                    }
+                }
+            }
+        }
+        // samples [L, L + R): positions window bi + 1 reads; store after it landed
+        if (more && !__all_sync(0xffffffffu, mbar_wait(bar, (bi + 1) & 1))) {
+            ok = false;
+            break;
+        }
+        if (va) {
+#pragma unroll
+            for (int i = L; i < L + R; ++i, d += ps) {
+                const int o = c + i - R;
+                if (inner || (unsigned)o < (unsigned)n) {
+                    const float2 v = s_get(P, i);
+                    if (ZL && !inner) ot = r_add(ot, v);
+                    put(d, v.x, v.y);
+                }
+            }
+        }
+    }
+    if (!ok) {
+        if (lane == 0) atomicExch(&g_rf_timeout, 1);
+        mbar_wait(bar, issued & 1);  // bounded: the copy still in flight, if any
+        return;
+    }
+    double *mass = J.mass;
+    double s_lk = r_warp_sum((double)(va ? lk.x : 0.0f) + (double)(vb ? lk.y : 0.0f));
+    if (!ZL) {
+        if (lane == 0 && s_lk != 0.0) atomicAdd(mass + MS_LEAK_Y, s_lk);
+    } else {
+        const double s_ot = r_warp_sum((double)(va ? ot.x : 0.0f) + (double)(vb ? ot.y : 0.0f));
+        const double lines = (double)min(max(nreal, 0), 64);
+        const double s_cv = s_ot / (double)keep - (double)b * n * lines;
+        s_lk = s_lk / (double)keep - (double)b * (2 * R) * lines;
+        if (lane == 0) {
+            if (s_lk != 0.0) atomicAdd(mass + MS_LEAK_Z, s_lk);
+            if (s_cv != 0.0) atomicAdd(mass + MS_CONV, s_cv);
+            if (s_ot != 0.0) atomicAdd(mass + MS_OUT, s_ot);
+        }
+    }
+}
+
+constexpr int RF_WIN_FLOATS = 64 * 64;  // one warp's window buffer
+
+// W warps per CTA, each on its own tile (tiles of other jobs than the CTA's
+// first are empty, as in rf_col_kernel); no CTA barrier after set-up.
+template <int W, bool ZL>
+__global__ void __launch_bounds__(32 * W, 12 / W) rf_col_tma_kernel(const OsJob *__restrict__ jobs,
+                                                                    const CUtensorMap *__restrict__ maps,
+                                                                    const OsTileInfo *__restrict__ tiles)
+{
+    extern __shared__ __align__(16) unsigned char rf_dyn[];
+    __shared__ __align__(16) float4 mt[64];
+    __shared__ __align__(8) uint64_t bars[W];
+    const int warp = threadIdx.x >> 5;
+    const int job = tiles[(size_t)blockIdx.x * W].job;
+    const OsTileInfo T = tiles[(size_t)blockIdx.x * W + warp];
+    const int nreal = T.job == job ? (T.flags & 255) : 0;
+    const OsJob &J = jobs[job];
+    if (threadIdx.x < W) mbar_init(&bars[threadIdx.x], 1);
+    if (threadIdx.x < W) mbar_fence_init();
+    s_fill_middle(mt, J.HH, threadIdx.x, 32 * W, ZL ? J.keep : 1.0f);
+    __syncthreads();
+    if (nreal == 0) return;
+    // window buffers on a 1024-byte boundary (the launch adds 1 KB of slack)
+    const uint32_t s0 = smem_u32(rf_dyn);
+    float *win = reinterpret_cast<float *>(rf_dyn + (((s0 + 1023u) & ~1023u) - s0)) + warp * RF_WIN_FLOATS;
+    const CUtensorMap *map = maps + job;
+    switch (J.r) {
+    case 1: rf_col_tma_body<1, ZL>(J, map, T, nreal, mt, win, &bars[warp]); break;
+    case 2: rf_col_tma_body<2, ZL>(J, map, T, nreal, mt, win, &bars[warp]); break;
+    case 3: rf_col_tma_body<3, ZL>(J, map, T, nreal, mt, win, &bars[warp]); break;
+    case 4: rf_col_tma_body<4, ZL>(J, map, T, nreal, mt, win, &bars[warp]); break;
+    case 5: rf_col_tma_body<5, ZL>(J, map, T, nreal, mt, win, &bars[warp]); break;
+    case 6: rf_col_tma_body<6, ZL>(J, map, T, nreal, mt, win, &bars[warp]); break;
+    case 7: rf_col_tma_body<7, ZL>(J, map, T, nreal, mt, win, &bars[warp]); break;
+    default: rf_col_tma_body<8, ZL>(J, map, T, nreal, mt, win, &bars[warp]); break;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // x pass: one warp = 64 rows (32 pairs).  Rows hold positions contiguously,
 // so blocks are moved through a shared tile with 16-byte copies:
 //   * chunks start on multiples of 4: the first output is -Rh (Rh = r
@@ -637,6 +831,210 @@ __global__ void __launch_bounds__(32, 12) rf_row_kernel(const OsJob *__restrict_
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// x pass with TMA staging.  Same blocks, tiles and register layout as
+// rf_row_body; the window of every block arrives by two 3D bulk tensor
+// copies (the field's rows seen as two tensors {nx, rows / 2} with row
+// stride 2 nx: even rows land in tile rows 0..31, odd rows in 32..63, the
+// conflict-free layout of rf_trow), one block ahead, into a per-warp input
+// tile; outputs go through a separate per-warp output tile to coalesced
+// 16-byte stores.  The last Rh outputs of a block (positions the next
+// window reads) are stored once that window has landed.
+// ---------------------------------------------------------------------------
+constexpr int RF_XTILE_FLOATS = 64 * RF_TS;  // one 64-row tile
+
+template <int R>
+__device__ __forceinline__ void rf_row_tma_body(const OsJob &J, const CUtensorMap *maps, const OsTileInfo &T,
+                                                const float4 *mt, float *IN, float *OUT, uint64_t *bar)
+{
+    constexpr int L = 64 - 2 * R;
+    constexpr int L4 = L & ~3;
+    constexpr int RH = (R + 3) & ~3;
+    constexpr int E = (RH - R) & ~1;
+    constexpr int R2 = RH - E;
+    constexpr int NST = (L4 - RH) / 4;
+    constexpr int NHD = RH / 4;
+    static_assert(R2 % 2 == 0 && R2 >= R && R2 + L4 - 1 + R <= 63, "x-pass block geometry");
+    const int lane = threadIdx.x & 31;
+    const int nreal = T.flags & 255;
+    const int n = J.n;
+    const int64_t ls = J.line_stride;
+    float *const base = J.data + (int64_t)T.l0 * ls;
+    const float b = J.b;
+    const bool masked = J.mask != 0;
+    bool in_a = 2 * lane < nreal, in_b = 2 * lane + 1 < nreal;
+    const bool va = in_a, vb = in_b;
+    int xlo = 0, xhi = n;
+    if (masked) {
+        xlo = J.box_lo[0];
+        xhi = J.box_hi[0];
+        if (va) {
+            const int rr = T.l0 + 2 * lane, y = rr % J.ny, z = rr / J.ny;
+            in_a = y >= J.box_lo[1] && y < J.box_hi[1] && z >= J.box_lo[2] && z < J.box_hi[2];
+        }
+        if (vb) {
+            const int rr = T.l0 + 2 * lane + 1, y = rr % J.ny, z = rr / J.ny;
+            in_b = y >= J.box_lo[1] && y < J.box_hi[1] && z >= J.box_lo[2] && z < J.box_hi[2];
+        }
+    }
+    const int nblocks = (n + R + RH + L4 - 1) / L4;
+    const int hw = lane >> 4, cq = lane & 15;
+    float *const rowp = base + (int64_t)hw * ls;
+    const int pair0 = T.l0 >> 1;  // first row pair of the tile
+    // window of block bi: positions [pa, pa + 68), pa = -2 Rh + bi L4 (a multiple of 4)
+    auto issue = [&](int bi) {
+        const int pa = -2 * RH + bi * L4;
+        mbar_arrive_expect_tx(bar, 64 * RF_TS * 4);
+        tma_load_3d(IN, maps, pa, pair0, 0, bar);                  // even rows
+        tma_load_3d(IN + 32 * RF_TS, maps + 1, pa, pair0, 0, bar);  // odd rows
+    };
+    // stores chunks [k0, k1) of every row's outputs from the output tile
+    auto store_chunks = [&](int c, int k0, int k1) {
+        const int k = k0 + cq;
+        const int o = c + 4 * k;
+        if (k < k1 && (unsigned)o < (unsigned)n) {
+            float *dst = rowp + o;
+            const float *src = OUT + (32 * hw) * RF_TS + 4 * k;
+            for (int r = hw; r < nreal; r += 2, dst += 2 * ls, src += RF_TS)
+                *reinterpret_cast<float4 *>(dst) = *reinterpret_cast<const float4 *>(src);
+        }
+    };
+    if (lane == 0) issue(0);
+    double acc_in = 0.0;
+    float2 lk = make_float2(0.0f, 0.0f);
+    int issued = 0;
+    bool ok = true;
+    for (int bi = 0; bi < nblocks; ++bi) {
+        const int c = -RH + bi * L4;  // first output, a multiple of 4
+        if (!__all_sync(0xffffffffu, mbar_wait(bar, bi & 1))) {
+            ok = false;
+            break;
+        }
+        sp2 P[32];
+        {
+            const float4 *ra = reinterpret_cast<const float4 *>(IN + lane * RF_TS);
+            const float4 *rb = reinterpret_cast<const float4 *>(IN + (32 + lane) * RF_TS);
+#pragma unroll
+            for (int m = 0; m < 17; ++m) {
+                const int j0 = (4 * m - E) / 2;
+                if (j0 + 1 < 0 || j0 >= 32) continue;
+                const float4 u = ra[m], w = rb[m];
+                if (j0 >= 0) P[j0] = sp2{make_float2(u.x, u.y), make_float2(w.x, w.y)};
+                if (j0 + 1 < 32) P[j0 + 1] = sp2{make_float2(u.z, u.w), make_float2(w.z, w.w)};
+            }
+        }
+        __syncwarp();
+        const bool more = bi + 1 < nblocks;
+        if (more && lane == 0) {
+            fence_proxy_async_smem();
+            issue(bi + 1);
+        }
+        if (more) issued = bi + 1;
+        if (!vb) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                P[j].im = make_float2(0.0f, 0.0f);
+                if (!va) P[j].re = make_float2(0.0f, 0.0f);
+            }
+        }
+        if (masked) {
+#pragma unroll
+            for (int i = 0; i < 64; ++i) {
+                const int p = c - R2 + i;
+                const bool px = p >= xlo && p < xhi;
+                float2 v = s_get(P, i);
+                v.x = (in_a && px) ? v.x - b : 0.0f;
+                v.y = (in_b && px) ? v.y - b : 0.0f;
+                s_set(P, i, v);
+            }
+        }
+        {
+            float2 sa = make_float2(0.0f, 0.0f), sb = sa;
+#pragma unroll
+            for (int j = R2 / 2; j < (R2 + L4) / 2; ++j) {
+                sa = r_add(sa, P[j].re);
+                sb = r_add(sb, P[j].im);
+            }
+            acc_in += (double)(va ? sa.x + sa.y : 0.0f) + (double)(vb ? sb.x + sb.y : 0.0f);
+        }
+        s_fft32_fwd(P);
+        s_middle(P, mt);
+        s_fft32_inv(P);
+#pragma unroll
+        for (int i = R2; i < R2 + L4; ++i) {
+            const int o = c + i - R2;
+            if (!((unsigned)o < (unsigned)n) && o >= -R && o < n + R) lk = r_add(lk, s_get(P, i));
+        }
+        {
+            float4 *wa = reinterpret_cast<float4 *>(OUT + lane * RF_TS);
+            float4 *wb = reinterpret_cast<float4 *>(OUT + (32 + lane) * RF_TS);
+#pragma unroll
+            for (int m = 0; m < L4 / 4; ++m) {
+                const int j = R2 / 2 + 2 * m;
+                wa[m] = make_float4(P[j].re.x, P[j].re.y, P[j + 1].re.x, P[j + 1].re.y);
+                wb[m] = make_float4(P[j].im.x, P[j].im.y, P[j + 1].im.x, P[j + 1].im.y);
+            }
+        }
+        __syncwarp();
+        store_chunks(c, 0, NST);
+        if (more && !__all_sync(0xffffffffu, mbar_wait(bar, (bi + 1) & 1))) {
+            ok = false;
+            break;
+        }
+        store_chunks(c, NST, NST + NHD);
+        __syncwarp();  // the output tile is rewritten by the next block
+    }
+    if (!ok) {
+        if (lane == 0) atomicExch(&g_rf_timeout, 1);
+        mbar_wait(bar, issued & 1);
+        return;
+    }
+    double *mass = J.mass;
+    const double s_in = r_warp_sum(acc_in);
+    const double s_lk = r_warp_sum((double)(va ? lk.x : 0.0f) + (double)(vb ? lk.y : 0.0f));
+    if (lane == 0) {
+        if (s_in != 0.0) atomicAdd(mass + MS_INPUT, s_in);
+        if (s_lk != 0.0) atomicAdd(mass + MS_LEAK_X, s_lk);
+    }
+}
+
+// W warps per CTA, each on its own 64-row tile (tiles of other jobs than the
+// CTA's first are empty); maps: two per job (even rows, odd rows).
+template <int W>
+__global__ void __launch_bounds__(32 * W, 6 / W) rf_row_tma_kernel(const OsJob *__restrict__ jobs,
+                                                                   const CUtensorMap *__restrict__ maps,
+                                                                   const OsTileInfo *__restrict__ tiles)
+{
+    extern __shared__ __align__(16) unsigned char rf_dyn[];
+    __shared__ __align__(16) float4 mt[64];
+    __shared__ __align__(8) uint64_t bars[W];
+    const int warp = threadIdx.x >> 5;
+    const int job = tiles[(size_t)blockIdx.x * W].job;
+    const OsTileInfo T = tiles[(size_t)blockIdx.x * W + warp];
+    const bool real = T.job == job && (T.flags & 255) > 0;
+    const OsJob &J = jobs[job];
+    if (threadIdx.x < W) mbar_init(&bars[threadIdx.x], 1);
+    if (threadIdx.x < W) mbar_fence_init();
+    s_fill_middle(mt, J.HH, threadIdx.x, 32 * W);
+    __syncthreads();
+    if (!real) return;
+    const uint32_t s0 = smem_u32(rf_dyn);
+    float *IN = reinterpret_cast<float *>(rf_dyn + (((s0 + 1023u) & ~1023u) - s0)) + warp * 2 * RF_XTILE_FLOATS;
+    float *OUT = IN + RF_XTILE_FLOATS;
+    const CUtensorMap *m = maps + 2 * job;
+    switch (J.r) {
+    case 1: rf_row_tma_body<1>(J, m, T, mt, IN, OUT, &bars[warp]); break;
+    case 2: rf_row_tma_body<2>(J, m, T, mt, IN, OUT, &bars[warp]); break;
+    case 3: rf_row_tma_body<3>(J, m, T, mt, IN, OUT, &bars[warp]); break;
+    case 4: rf_row_tma_body<4>(J, m, T, mt, IN, OUT, &bars[warp]); break;
+    case 5: rf_row_tma_body<5>(J, m, T, mt, IN, OUT, &bars[warp]); break;
+    case 6: rf_row_tma_body<6>(J, m, T, mt, IN, OUT, &bars[warp]); break;
+    case 7: rf_row_tma_body<7>(J, m, T, mt, IN, OUT, &bars[warp]); break;
+    default: rf_row_tma_body<8>(J, m, T, mt, IN, OUT, &bars[warp]); break;
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -678,8 +1076,8 @@ static bool rf_row_enabled()
 
 // Warps per CTA of the y/z kernel (VFD_RF_W: 1, 2, 4, 6 or 12; default 4:
 // on B200 the 512x256x384 world's y and z passes took 0.737 / 0.761 ms with
-// 4, 0.766 / 0.794 with 1, 0.768 / 0.775 with 12); the x kernel takes one
-// warp per CTA.
+// 4, 0.766 / 0.794 with 1, 0.768 / 0.775 with 12); the x kernel takes two
+// warps per CTA when its windows are staged by TMA, else one.
 int rf_cta_warps(int axis)
 {
     static int w = -1;
@@ -688,7 +1086,8 @@ int rf_cta_warps(int axis)
         const int v = e ? atoi(e) : 4;
         w = (v == 1 || v == 2 || v == 4 || v == 6 || v == 12) ? v : 4;
     }
-    return axis == PASS_X ? 1 : w;
+    if (axis == PASS_X) return rf_tma_enabled() && rf_row_enabled() ? 2 : 1;
+    return w;
 }
 
 static std::mutex g_rf_mu;
@@ -722,7 +1121,73 @@ cudaError_t rf_prepare()
     return e;
 }
 
-cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int axis, cudaStream_t st)
+bool rf_take_timeout()
+{
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_rf_timeout, sizeof(int)) != cudaSuccess) return false;
+    if (v) {
+        const int z = 0;
+        cudaMemcpyToSymbol(g_rf_timeout, &z, sizeof(int));
+    }
+    return v != 0;
+}
+
+// VFD_RF_TMA=0 keeps the y and z passes on direct global loads.
+bool rf_tma_enabled()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("VFD_RF_TMA");
+        on = (e && e[0] == '0') ? 0 : 1;
+    }
+    return on == 1 && tma_available();
+}
+
+bool rf_encode_map(const OsJob &j, CUtensorMap *m)
+{
+    if (j.kind == PASS_X) {
+        // rows of n positions, row stride line_stride: even rows and odd rows
+        // as two tensors {n, rows / 2} with row stride 2 line_stride
+        const uint64_t n = (uint64_t)j.n, rows = (uint64_t)j.nlines * j.nouter;
+        const uint64_t rs = (uint64_t)j.line_stride * 4;
+        if (j.nouter != 1 || rows < 2 || (j.n & 3) != 0 || (rs & 15) != 0) return false;
+        const uint64_t ne = (rows + 1) / 2, no = rows / 2;
+        return tma_encode_3d(&m[0], j.data, n, ne, 1, 2 * rs, 2 * rs * ne, RF_TS, 32, 1) &&
+               tma_encode_3d(&m[1], j.data + j.line_stride, n, no, 1, 2 * rs, 2 * rs * no, RF_TS, 32, 1);
+    }
+    if (j.line_stride != 1) return false;
+    // the field as the tensor {nx, ny, nz}: y pass (lines x, positions y,
+    // outer z), z pass (lines x, outer y, positions z)
+    const uint64_t nx = (uint64_t)j.nlines;
+    const uint64_t ny = j.kind == PASS_Y ? (uint64_t)j.n : (uint64_t)j.nouter;
+    const uint64_t nz = j.kind == PASS_Y ? (uint64_t)j.nouter : (uint64_t)j.n;
+    const uint64_t sy = (uint64_t)(j.kind == PASS_Y ? j.pos_stride : j.outer_stride) * 4;
+    const uint64_t sz = (uint64_t)(j.kind == PASS_Y ? j.outer_stride : j.pos_stride) * 4;
+    if (sy != nx * 4 || sz != nx * ny * 4) return false;
+    if (j.kind == PASS_Y) return tma_encode_3d(m, j.data, nx, ny, nz, sy, sz, 64, 64, 1);
+    return tma_encode_3d(m, j.data, nx, ny, nz, sy, sz, 64, 1, 64);
+}
+
+template <int W, bool Z>
+static cudaError_t launch_col_tma(const OsJob *jobs, const CUtensorMap *maps, const OsTileInfo *tiles, int nb,
+                                  cudaStream_t st)
+{
+    const size_t dyn = (size_t)W * RF_WIN_FLOATS * sizeof(float) + 1024;
+    static int done[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        e = cudaFuncSetAttribute(rf_col_tma_kernel<W, Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        if (e != cudaSuccess) return e;
+        done[dev] = 1;
+    }
+    rf_col_tma_kernel<W, Z><<<nb, 32 * W, dyn, st>>>(jobs, maps, tiles);
+    return cudaSuccess;
+}
+
+cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int axis, cudaStream_t st,
+                      const CUtensorMap *maps)
 {
     if (ntiles <= 0) return cudaSuccess;
     int dev = 0;
@@ -737,8 +1202,21 @@ cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, in
     const int W = rf_cta_warps(axis);
     if (ntiles % W != 0) return cudaErrorInvalidValue;
     const int nb = ntiles / W;
-    if (axis == PASS_X) {
+    if (axis == PASS_X && maps && W == 2) {
+        const size_t dyn = (size_t)2 * 2 * RF_XTILE_FLOATS * sizeof(float) + 1024;
+        static int done[64] = {};
+        if (dev >= 0 && dev < 64 && !done[dev]) {
+            e = cudaFuncSetAttribute(rf_row_tma_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+            if (e != cudaSuccess) return e;
+            done[dev] = 1;
+        }
+        rf_row_tma_kernel<2><<<nb, 64, dyn, st>>>(jobs, maps, tiles);
+    } else if (axis == PASS_X) {
         rf_row_kernel<<<ntiles, 32, 0, st>>>(jobs, tiles);
+    } else if (maps && W == 4) {
+        e = axis == PASS_Z ? launch_col_tma<4, true>(jobs, maps, tiles, nb, st)
+                           : launch_col_tma<4, false>(jobs, maps, tiles, nb, st);
+        if (e != cudaSuccess) return e;
     } else {
         const bool z = axis == PASS_Z;
         switch (W) {

@@ -2,6 +2,7 @@
 // (vfd_rf.cu).  Jobs are overlap-save jobs (vfd_os.h) of radius <= RF_RMAX;
 // tiles are 64 lines.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -24,7 +25,18 @@ int rf_cta_warps(int axis);
 // Uploads the FFT-64 twiddles to the current device (outside stream capture).
 cudaError_t rf_prepare();
 // One launch over `ntiles` tiles of jobs (any radius <= RF_RMAX) that all
-// belong to `axis`.
-cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int axis, cudaStream_t st);
+// belong to `axis`.  maps (y / z passes): one TMA tensor map per job, indexed
+// like `jobs`; the windows are then staged by bulk tensor copies.
+cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int axis, cudaStream_t st,
+                      const CUtensorMap *maps = nullptr);
+// Whether the y / z passes stage their windows with TMA (VFD_RF_TMA=0: no).
+bool rf_tma_enabled();
+// Encodes job j's tensor maps for a TMA-staged launch (x pass: two, m[0]
+// and m[1]; y / z: one); false if the job's layout does not allow it (then
+// the launch uses the kernels without TMA).
+bool rf_encode_map(const OsJob &j, CUtensorMap *m);
+// Reads and clears the flag a pass sets when a bounded wait for a bulk copy
+// gave up.
+bool rf_take_timeout();
 
 }  // namespace vfd

@@ -204,6 +204,7 @@ struct RfGroup {
     int r = 0;  // unused: the kernel reads each tile's radius from its job
     int ntiles = 0;
     OsTileInfo *d_tiles = nullptr;
+    CUtensorMap *d_maps = nullptr;  // y / z: one TMA map per job (NULL: direct loads)
 };
 
 static bool rf_enabled()
@@ -242,10 +243,26 @@ static cudaError_t build_rf_groups(const OsJob *jobs, int n, std::vector<RfGroup
     RfGroup g;
     g.r = 0;
     g.ntiles = (int)t.size();
+    // TMA tensor maps (x: two per job, y / z: one) when every job's layout
+    // allows them; the CTA widths the TMA kernels take (x 2 warps, y / z 4)
+    std::vector<CUtensorMap> maps;
+    const bool xpass = jobs[0].kind == PASS_X;
+    const int per = xpass ? 2 : 1;
+    if (rf_tma_enabled() && W == (xpass ? 2 : 4)) {
+        maps.resize((size_t)n * per);
+        for (int i = 0; i < n && !maps.empty(); ++i)
+            if (!rf_encode_map(jobs[i], &maps[(size_t)i * per])) maps.clear();
+    }
     cudaError_t e = cudaMalloc(&g.d_tiles, sizeof(OsTileInfo) * t.size());
     if (e == cudaSuccess) e = cudaMemcpy(g.d_tiles, t.data(), sizeof(OsTileInfo) * t.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !maps.empty()) {
+        e = cudaMalloc(&g.d_maps, sizeof(CUtensorMap) * maps.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpy(g.d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice);
+    }
     if (e != cudaSuccess) {
         cudaFree(g.d_tiles);
+        cudaFree(g.d_maps);
         return e;
     }
     out.push_back(g);
@@ -254,14 +271,17 @@ static cudaError_t build_rf_groups(const OsJob *jobs, int n, std::vector<RfGroup
 
 static void free_rf_groups(std::vector<RfGroup> &g)
 {
-    for (auto &x : g) cudaFree(x.d_tiles);
+    for (auto &x : g) {
+        cudaFree(x.d_tiles);
+        cudaFree(x.d_maps);
+    }
     g.clear();
 }
 
 static cudaError_t launch_rf_groups(const OsJob *jobs, const std::vector<RfGroup> &g, int axis, cudaStream_t st)
 {
     for (const auto &x : g) {
-        cudaError_t e = launch_rf(jobs, x.d_tiles, x.ntiles, axis, st);
+        cudaError_t e = launch_rf(jobs, x.d_tiles, x.ntiles, axis, st, x.d_maps);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -1456,6 +1476,7 @@ vfd_status vfd_read_mass(vfd_world *w, vfd_mass *out, void *stream)
         out[f].reserved = 0.0;
     }
     if (herr) return fail(w, VFD_ERR_DEVICE_FAULT, "a kernel rejected an out-of-range index");
+    if (rf_take_timeout()) return fail(w, VFD_ERR_TIMEOUT, "an axis pass gave up waiting for a bulk copy");
     return VFD_OK;
 }
 
