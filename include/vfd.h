@@ -277,6 +277,13 @@ vfd_status vfd_diffuse_update_host(vfd_world *w, float *const *host_p, float *co
 typedef struct vfd_batch vfd_batch;
 vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **out);
 vfd_status vfd_batch_tick(vfd_batch *b, int n_substeps, void *stream);
+/* Per-axis pass choice for the batch as a whole: times every candidate
+ * (register FFT, overlap-save at 3 and at 4 resident CTAs per SM, full-line
+ * FFT) over all the batch's fields -- one warm-up and `reps` timed launches
+ * each, CUDA events -- and keeps the fastest per axis (out3, may be NULL).
+ * The passes run on the worlds' own fields, which are saved to temporary
+ * device buffers and restored.  The next tick re-captures the graph. */
+vfd_status vfd_batch_autotune(vfd_batch *b, int reps, vfd_axis_tuning *out3);
 vfd_status vfd_batch_destroy(vfd_batch *b);
 const char *vfd_batch_last_error(const vfd_batch *b);
 
@@ -286,8 +293,13 @@ const char *vfd_batch_last_error(const vfd_batch *b);
  * request's device bytes fit hbm_budget_bytes; admitted fields stay resident
  * on the device for all the request's ticks.  Each round advances every
  * active request by one tick (substeps_per_tick substeps) with all their
- * fields in one launch per axis pass; finished requests are retired (totals,
- * optional download) and free their slot and memory for the next admission.
+ * fields in one launch per axis pass; up to three rounds are queued on the
+ * device at a time, so the host prepares the next rounds (admissions, batch
+ * set-up) while the device works.  Finished requests are retired (totals,
+ * optional download) once their last round has completed and free their
+ * slot; their device memory is returned in bulk (device memory is freed
+ * while the device is idle, or when the budget needs it, since freeing waits
+ * for the device).
  * A request's results do not depend on which other requests share its
  * rounds (each field's lines stay in their own tiles).
  * Host buffers named by a request (init, result, mass) must stay valid until
@@ -321,9 +333,14 @@ typedef struct vfd_server_stats {
     int64_t submitted, admitted, completed, rejected, active, queued, rounds;
     double busy_s;                      /* time with at least one active request */
     double voxel_steps_done;
-    double p50_latency_s, p99_latency_s, mean_latency_s;  /* submit -> done   */
+    /* submit -> done over every submitted request: one still queued or
+     * resident counts with the time it has waited so far (a lower bound of
+     * its latency; `censored` of them) */
+    double p50_latency_s, p99_latency_s, mean_latency_s;
     size_t hbm_in_use, hbm_peak;
     double device_s;                    /* device time of the rounds (CUDA events) */
+    double p50_completed_s, p99_completed_s;  /* over completed requests only */
+    int64_t censored;
 } vfd_server_stats;
 
 vfd_status vfd_server_create(int device, size_t hbm_budget_bytes, int max_active, int substeps_per_tick,

@@ -100,3 +100,30 @@ def test_single_world_is_deterministic(gpu, grid, sig):
         w.close()
     for f in range(3):
         np.testing.assert_array_equal(outs[0][f], outs[1][f])
+
+
+def test_batch_autotune_keeps_fields_and_results(gpu):
+    """vfd_batch_autotune times the pass candidates on the worlds' own fields
+    and restores them: ticks after tuning equal ticks of untuned single worlds."""
+    specs = [((96, 64, 64), [1.0, 2.1, 0.6]), ((70, 33, 41), [1.7, 0.5, 1.2]), ((128, 96, 96), [0.9, 1.3, 2.4])]
+    dec = [0.05, 0.01, 0.03]
+    worlds, singles = [], []
+    for i, (g, sig) in enumerate(specs):
+        worlds.append(make_world(g, sig, dec, 2, i)[0])
+        singles.append(make_world(g, sig, dec, 2, i)[0])
+    before = [w.download(0).copy() for w in worlds]
+    with vfd.Batch(worlds) as b:
+        tuning = b.autotune(reps=2)
+        assert len(tuning) == 3 and all(t["ms"] > 0 for t in tuning)
+        for w, u in zip(worlds, before):
+            np.testing.assert_array_equal(w.download(0), u)
+        for _ in range(3):
+            b.tick(2)
+    for s in singles:
+        for _ in range(3):
+            s.tick(2)
+    for w, s in zip(worlds, singles):
+        for f in range(3):
+            assert rel_l2(w.download(f), s.download(f)) <= 1e-6
+    for w in worlds + singles:
+        w.close()

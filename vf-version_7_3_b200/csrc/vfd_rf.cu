@@ -838,11 +838,15 @@ __global__ void __launch_bounds__(32, 12) rf_row_kernel(const OsJob *__restrict_
 // copies (the field's rows seen as two tensors {nx, rows / 2} with row
 // stride 2 nx: even rows land in tile rows 0..31, odd rows in 32..63, the
 // conflict-free layout of rf_trow), one block ahead, into a per-warp input
-// tile; outputs go through a separate per-warp output tile to coalesced
-// 16-byte stores.  The last Rh outputs of a block (positions the next
-// window reads) are stored once that window has landed.
+// tile.  Outputs go to global memory through a per-warp 32-row output tile,
+// even rows then odd rows, as coalesced 16-byte stores; they are stored once
+// the next window has landed, because its first Rh positions are this
+// block's last outputs.  26 KB of shared memory per warp: 8 warps per SM.
 // ---------------------------------------------------------------------------
-constexpr int RF_XTILE_FLOATS = 64 * RF_TS;  // one 64-row tile
+constexpr int RF_XTILE_FLOATS = 64 * RF_TS;        // the 64-row input tile
+constexpr int RF_XOUT_FLOATS = 32 * RF_TS;         // the 32-row output tile
+constexpr int RF_XWARP_BYTES = 26 * 1024;          // per-warp stride (input + output tiles, 1 KB aligned)
+static_assert((RF_XTILE_FLOATS + RF_XOUT_FLOATS) * 4 <= RF_XWARP_BYTES, "x-pass tiles");
 
 template <int R>
 __device__ __forceinline__ void rf_row_tma_body(const OsJob &J, const CUtensorMap *maps, const OsTileInfo &T,
@@ -853,9 +857,8 @@ __device__ __forceinline__ void rf_row_tma_body(const OsJob &J, const CUtensorMa
     constexpr int RH = (R + 3) & ~3;
     constexpr int E = (RH - R) & ~1;
     constexpr int R2 = RH - E;
-    constexpr int NST = (L4 - RH) / 4;
-    constexpr int NHD = RH / 4;
     static_assert(R2 % 2 == 0 && R2 >= R && R2 + L4 - 1 + R <= 63, "x-pass block geometry");
+    static_assert(L4 / 4 <= 16, "one chunk per lane of a half-warp");
     const int lane = threadIdx.x & 31;
     const int nreal = T.flags & 255;
     const int n = J.n;
@@ -880,7 +883,6 @@ __device__ __forceinline__ void rf_row_tma_body(const OsJob &J, const CUtensorMa
     }
     const int nblocks = (n + R + RH + L4 - 1) / L4;
     const int hw = lane >> 4, cq = lane & 15;
-    float *const rowp = base + (int64_t)hw * ls;
     const int pair0 = T.l0 >> 1;  // first row pair of the tile
     // window of block bi: positions [pa, pa + 68), pa = -2 Rh + bi L4 (a multiple of 4)
     auto issue = [&](int bi) {
@@ -889,14 +891,15 @@ __device__ __forceinline__ void rf_row_tma_body(const OsJob &J, const CUtensorMa
         tma_load_3d(IN, maps, pa, pair0, 0, bar);                  // even rows
         tma_load_3d(IN + 32 * RF_TS, maps + 1, pa, pair0, 0, bar);  // odd rows
     };
-    // stores chunks [k0, k1) of every row's outputs from the output tile
-    auto store_chunks = [&](int c, int k0, int k1) {
-        const int k = k0 + cq;
-        const int o = c + 4 * k;
-        if (k < k1 && (unsigned)o < (unsigned)n) {
-            float *dst = rowp + o;
-            const float *src = OUT + (32 * hw) * RF_TS + 4 * k;
-            for (int r = hw; r < nreal; r += 2, dst += 2 * ls, src += RF_TS)
+    // stores the block's outputs of the rows of parity `par` (tile row t =
+    // line row 2t + par) from the output tile: half-warp hw takes t = hw,
+    // hw + 2, ..., lane cq the 16-byte chunk cq of each
+    auto store_rows = [&](int c, int par) {
+        const int o = c + 4 * cq;
+        if (cq < L4 / 4 && (unsigned)o < (unsigned)n) {
+            float *dst = base + (int64_t)(2 * hw + par) * ls + o;
+            const float *src = OUT + hw * RF_TS + 4 * cq;
+            for (int t = hw; 2 * t + par < nreal; t += 2, dst += 4 * ls, src += 2 * RF_TS)
                 *reinterpret_cast<float4 *>(dst) = *reinterpret_cast<const float4 *>(src);
         }
     };
@@ -966,23 +969,32 @@ __device__ __forceinline__ void rf_row_tma_body(const OsJob &J, const CUtensorMa
             const int o = c + i - R2;
             if (!((unsigned)o < (unsigned)n) && o >= -R && o < n + R) lk = r_add(lk, s_get(P, i));
         }
-        {
-            float4 *wa = reinterpret_cast<float4 *>(OUT + lane * RF_TS);
-            float4 *wb = reinterpret_cast<float4 *>(OUT + (32 + lane) * RF_TS);
-#pragma unroll
-            for (int m = 0; m < L4 / 4; ++m) {
-                const int j = R2 / 2 + 2 * m;
-                wa[m] = make_float4(P[j].re.x, P[j].re.y, P[j + 1].re.x, P[j + 1].re.y);
-                wb[m] = make_float4(P[j].im.x, P[j].im.y, P[j + 1].im.x, P[j + 1].im.y);
-            }
-        }
-        __syncwarp();
-        store_chunks(c, 0, NST);
+        // the next window holds this block's last Rh outputs' positions
         if (more && !__all_sync(0xffffffffu, mbar_wait(bar, (bi + 1) & 1))) {
             ok = false;
             break;
         }
-        store_chunks(c, NST, NST + NHD);
+        {
+            float4 *wa = reinterpret_cast<float4 *>(OUT + lane * RF_TS);
+#pragma unroll
+            for (int m = 0; m < L4 / 4; ++m) {
+                const int j = R2 / 2 + 2 * m;
+                wa[m] = make_float4(P[j].re.x, P[j].re.y, P[j + 1].re.x, P[j + 1].re.y);
+            }
+        }
+        __syncwarp();
+        store_rows(c, 0);
+        __syncwarp();
+        {
+            float4 *wb = reinterpret_cast<float4 *>(OUT + lane * RF_TS);
+#pragma unroll
+            for (int m = 0; m < L4 / 4; ++m) {
+                const int j = R2 / 2 + 2 * m;
+                wb[m] = make_float4(P[j].im.x, P[j].im.y, P[j + 1].im.x, P[j + 1].im.y);
+            }
+        }
+        __syncwarp();
+        store_rows(c, 1);
         __syncwarp();  // the output tile is rewritten by the next block
     }
     if (!ok) {
@@ -1002,7 +1014,7 @@ __device__ __forceinline__ void rf_row_tma_body(const OsJob &J, const CUtensorMa
 // W warps per CTA, each on its own 64-row tile (tiles of other jobs than the
 // CTA's first are empty); maps: two per job (even rows, odd rows).
 template <int W>
-__global__ void __launch_bounds__(32 * W, 6 / W) rf_row_tma_kernel(const OsJob *__restrict__ jobs,
+__global__ void __launch_bounds__(32 * W, 8 / W) rf_row_tma_kernel(const OsJob *__restrict__ jobs,
                                                                    const CUtensorMap *__restrict__ maps,
                                                                    const OsTileInfo *__restrict__ tiles)
 {
@@ -1020,7 +1032,7 @@ __global__ void __launch_bounds__(32 * W, 6 / W) rf_row_tma_kernel(const OsJob *
     __syncthreads();
     if (!real) return;
     const uint32_t s0 = smem_u32(rf_dyn);
-    float *IN = reinterpret_cast<float *>(rf_dyn + (((s0 + 1023u) & ~1023u) - s0)) + warp * 2 * RF_XTILE_FLOATS;
+    float *IN = reinterpret_cast<float *>(rf_dyn + (((s0 + 1023u) & ~1023u) - s0) + warp * RF_XWARP_BYTES);
     float *OUT = IN + RF_XTILE_FLOATS;
     const CUtensorMap *m = maps + 2 * job;
     switch (J.r) {
@@ -1203,7 +1215,7 @@ cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, in
     if (ntiles % W != 0) return cudaErrorInvalidValue;
     const int nb = ntiles / W;
     if (axis == PASS_X && maps && W == 2) {
-        const size_t dyn = (size_t)2 * 2 * RF_XTILE_FLOATS * sizeof(float) + 1024;
+        const size_t dyn = (size_t)2 * RF_XWARP_BYTES + 1024;
         static int done[64] = {};
         if (dev >= 0 && dev < 64 && !done[dev]) {
             e = cudaFuncSetAttribute(rf_row_tma_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);

@@ -5,15 +5,21 @@
 //   * admission, FIFO: the head request is admitted while the active set has
 //     a free slot and its device bytes fit the HBM budget; its fields are
 //     created resident (host upload or the device generator) and stay on the
-//     device for all its ticks;
+//     device for all its ticks.  A world retired by an earlier request of the
+//     same shape and parameters is reused (fields and sources re-initialised),
+//     so a steady stream of requests allocates no device memory;
 //   * a round advances every active request by one tick: all their fields go
 //     through one launch per axis pass per substep (vfd_batch, replayed as a
 //     CUDA graph while the active set is unchanged);
-//   * while a round runs, the requests finishing with it are known: new
-//     arrivals are admitted into their slots and the next round's batch is
-//     built on the host; after the round the finished requests are retired
-//     (totals, optional download) and their memory is freed, so new arrivals
-//     join while others are still on the device.
+//   * up to kRoundsInFlight rounds are queued on the device: the set of the
+//     next round is known when a round is launched (every request's tick
+//     count is), so the host admits arrivals and builds the next batch while
+//     earlier rounds run.  A request is retired (totals, optional download)
+//     once the round holding its last tick has completed, on a stream of its
+//     own, and its slot is free for the next admission;
+//   * device memory is freed only while no round is in flight (freeing waits
+//     for the device): retired worlds wait in a pool for reuse and are freed
+//     when the device is idle or the budget needs their bytes.
 // The reference has no serving layer: it diffuses one world per tick from
 // WHWorld::go (woundHealingWorld.cpp:2013-2026).
 #include <cuda_runtime.h>
@@ -34,6 +40,8 @@
 
 namespace {
 
+constexpr int kRoundsInFlight = 3;
+
 struct Request {
     uint64_t id = 0;
     // copies of the description
@@ -50,12 +58,27 @@ struct Request {
     // state
     vfd_world *world = nullptr;
     size_t bytes = 0;
-    int ticks_done = 0;
+    int ticks_launched = 0;
     vfd_request_info info;
     std::string err;
 };
 
 double latency_of(const vfd_request_info &i) { return i.t_done - i.t_submit; }
+
+// One round queued on the device.
+struct Round {
+    cudaEvent_t start = nullptr, end = nullptr;
+    std::vector<std::shared_ptr<Request>> finishing;  // requests whose last tick this round holds
+};
+
+// Worlds are reused by requests of the same shape and parameters.
+std::string world_key(const Request &r)
+{
+    std::string k(reinterpret_cast<const char *>(r.params.data()), r.params.size() * sizeof(vfd_field_params));
+    const int d[6] = {r.nx, r.ny, r.nz, r.nf, r.pad_mode, r.epi};
+    k.append(reinterpret_cast<const char *>(d), sizeof(d));
+    return k;
+}
 
 }  // namespace
 
@@ -70,6 +93,7 @@ struct vfd_server {
     std::condition_variable cv_work, cv_done;
     std::deque<std::shared_ptr<Request>> pending;
     std::map<uint64_t, std::shared_ptr<Request>> finished;
+    std::map<uint64_t, double> open_submit;  // submitted, not finished: submit time
     std::vector<double> latencies;
     uint64_t next_id = 1;
     bool stop = false;
@@ -78,13 +102,17 @@ struct vfd_server {
     double busy_since = -1.0;  // start of the current busy span (under mu)
 
     // scheduler-owned
-    std::vector<std::shared_ptr<Request>> active;
-    std::vector<std::pair<vfd_world *, size_t>> dead;  // retired worlds not yet destroyed
+    std::vector<std::shared_ptr<Request>> active;    // requests with ticks still to launch
+    std::deque<Round> inflight;
+    std::vector<cudaEvent_t> ev_pool;
+    std::multimap<std::string, std::pair<vfd_world *, size_t>> pool;  // retired worlds, by key
+    size_t pool_bytes = 0;
+    std::vector<vfd_batch *> dead_batches;           // replaced batches, destroyed while idle
     vfd_batch *batch = nullptr;
     bool set_changed = true;
-    size_t in_use = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev_round[2] = {nullptr, nullptr};  // brackets each round on `stream`
+    size_t in_use = 0;                               // active + retiring + pooled world bytes
+    cudaStream_t stream = nullptr;                   // rounds
+    cudaStream_t rstream = nullptr;                  // retirement reads
     std::thread worker;
     std::string err;
 
@@ -112,6 +140,7 @@ void finish(vfd_server *s, const std::shared_ptr<Request> &r, int status, const 
     r->err = msg;
     std::lock_guard<std::mutex> lk(s->mu);
     s->finished[r->id] = r;
+    s->open_submit.erase(r->id);
     if (status == VFD_OK) {
         s->st.completed++;
         s->st.voxel_steps_done += r->info.voxel_steps;
@@ -122,25 +151,22 @@ void finish(vfd_server *s, const std::shared_ptr<Request> &r, int status, const 
     s->cv_done.notify_all();
 }
 
-// Creates the request's world on the device (scheduler thread).
-int admit(vfd_server *s, const std::shared_ptr<Request> &r, std::string &msg)
+cudaEvent_t take_event(vfd_server *s)
 {
-    vfd_world_desc d;
-    d.nx = r->nx;
-    d.ny = r->ny;
-    d.nz = r->nz;
-    d.n_fields = r->nf;
-    d.fields = r->params.data();
-    d.pad_mode = r->pad_mode;
-    d.epi_boundary = r->epi;
-    d.fft[0] = d.fft[1] = d.fft[2] = 0;
-    d.method = VFD_METHOD_SEPARABLE;
-    vfd_status st = vfd_world_create(&d, s->device, &r->world);
-    if (st != VFD_OK) {
-        msg = vfd_last_error(nullptr);
-        r->world = nullptr;
-        return st;
+    if (!s->ev_pool.empty()) {
+        cudaEvent_t e = s->ev_pool.back();
+        s->ev_pool.pop_back();
+        return e;
     }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Fills the request's fields and sources into its world.
+int fill(vfd_server *s, const std::shared_ptr<Request> &r)
+{
+    vfd_status st = VFD_OK;
     for (int f = 0; f < r->nf && st == VFD_OK; ++f) {
         if (!r->init.empty()) {
             st = vfd_upload_field(r->world, f, r->init[f], s->stream);
@@ -151,14 +177,59 @@ int admit(vfd_server *s, const std::shared_ptr<Request> &r, std::string &msg)
                 st = vfd_synth_field_device(r->seed, r->synth_world, f, r->lo, r->hi, p,
                                             (size_t)r->nx * r->ny * r->nz, s->stream);
         }
-        if (st == VFD_OK && !r->src_idx.empty())
-            st = vfd_set_sources(r->world, f, r->src_idx[f].data(), r->src_amt[f].data(),
-                                 (int64_t)r->src_idx[f].size());
+        if (st == VFD_OK) {
+            const bool has = !r->src_idx.empty();
+            st = vfd_set_sources(r->world, f, has ? r->src_idx[f].data() : nullptr,
+                                 has ? r->src_amt[f].data() : nullptr, has ? (int64_t)r->src_idx[f].size() : 0);
+        }
     }
-    if (st == VFD_OK) st = vfd_world_device_bytes(r->world, &r->bytes);
+    return st;
+}
+
+// Puts the request's world on the device: a pooled world of the same key, or
+// a new one (scheduler thread).  `reused` tells which.
+int admit(vfd_server *s, const std::shared_ptr<Request> &r, bool *reused, std::string &msg)
+{
+    *reused = false;
+    auto it = s->pool.find(world_key(*r));
+    if (it != s->pool.end()) {
+        r->world = it->second.first;
+        r->bytes = it->second.second;
+        s->pool_bytes -= r->bytes;
+        s->pool.erase(it);
+        *reused = true;
+    } else {
+        vfd_world_desc d;
+        d.nx = r->nx;
+        d.ny = r->ny;
+        d.nz = r->nz;
+        d.n_fields = r->nf;
+        d.fields = r->params.data();
+        d.pad_mode = r->pad_mode;
+        d.epi_boundary = r->epi;
+        d.fft[0] = d.fft[1] = d.fft[2] = 0;
+        d.method = VFD_METHOD_SEPARABLE;
+        vfd_status st = vfd_world_create(&d, s->device, &r->world);
+        if (st != VFD_OK) {
+            msg = vfd_last_error(nullptr);
+            r->world = nullptr;
+            return st;
+        }
+        if ((st = vfd_world_device_bytes(r->world, &r->bytes)) != VFD_OK) {
+            msg = vfd_last_error(r->world);
+            vfd_world_destroy(r->world);
+            r->world = nullptr;
+            return st;
+        }
+    }
+    const int st = fill(s, r);
     if (st != VFD_OK) {
         msg = vfd_last_error(r->world);
-        vfd_world_destroy(r->world);
+        if (*reused) {
+            s->in_use -= r->bytes;  // a pooled world's bytes were counted already
+            *reused = false;
+        }
+        vfd_world_destroy(r->world);  // only reached with no round using this world
         r->world = nullptr;
         return st;
     }
@@ -167,41 +238,82 @@ int admit(vfd_server *s, const std::shared_ptr<Request> &r, std::string &msg)
     return VFD_OK;
 }
 
-// Reads a finished request's results; its world is destroyed later (`dead`),
-// after the next round has been launched, because freeing device memory
-// waits for the device.
+// Reads a finished request's results (its last round has completed); its
+// world goes to the pool.
 int retire(vfd_server *s, const std::shared_ptr<Request> &r, std::string &msg)
 {
     int st = VFD_OK;
-    if (r->mass) st = vfd_read_mass(r->world, r->mass, s->stream);
+    if (r->mass) st = vfd_read_mass(r->world, r->mass, s->rstream);
     for (int f = 0; f < r->nf && st == VFD_OK && !r->result.empty(); ++f)
-        if (r->result[f]) st = vfd_download_field(r->world, f, r->result[f], s->stream);
+        if (r->result[f]) st = vfd_download_field(r->world, f, r->result[f], s->rstream);
     if (st != VFD_OK) msg = vfd_last_error(r->world);
-    s->dead.push_back({r->world, r->bytes});
+    s->pool.insert({world_key(*r), {r->world, r->bytes}});
+    s->pool_bytes += r->bytes;
     r->world = nullptr;
     return st;
 }
 
-// Destroys the worlds of retired requests and returns their memory to the budget.
-void bury(vfd_server *s)
+// Waits for the oldest round in flight, accounts its device time and retires
+// the requests it finished.
+void complete_oldest(vfd_server *s)
 {
-    if (s->dead.empty()) return;
-    for (auto &d : s->dead) {
-        vfd_world_destroy(d.first);
-        s->in_use -= d.second;
+    Round rd = std::move(s->inflight.front());
+    s->inflight.pop_front();
+    float ms = 0.0f;
+    const bool ok = cudaEventSynchronize(rd.end) == cudaSuccess;
+    if (ok) cudaEventElapsedTime(&ms, rd.start, rd.end);
+    s->ev_pool.push_back(rd.start);
+    s->ev_pool.push_back(rd.end);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->st.rounds++;
+        s->st.device_s += 1e-3 * ms;
     }
-    s->dead.clear();
+    for (auto &r : rd.finishing) {
+        std::string msg;
+        const int st = ok ? retire(s, r, msg) : VFD_ERR_CUDA;
+        if (!ok) {
+            msg = "a round failed on the device";
+            s->pool.insert({world_key(*r), {r->world, r->bytes}});
+            s->pool_bytes += r->bytes;
+            r->world = nullptr;
+        }
+        finish(s, r, st, msg);
+    }
+}
+
+void complete_all(vfd_server *s)
+{
+    while (!s->inflight.empty()) complete_oldest(s);
+}
+
+// Frees pooled worlds and replaced batches; only with no round in flight.
+void free_idle(vfd_server *s)
+{
+    complete_all(s);
+    for (auto *b : s->dead_batches) vfd_batch_destroy(b);
+    s->dead_batches.clear();
+    for (auto &kv : s->pool) {
+        vfd_world_destroy(kv.second.first);
+        s->in_use -= kv.second.second;
+    }
+    s->pool.clear();
+    s->pool_bytes = 0;
     std::lock_guard<std::mutex> lk(s->mu);
     s->st.hbm_in_use = s->in_use;
 }
 
 // Takes requests off the queue while slots and budget allow (FIFO; a request
-// larger than the whole budget is rejected).  `occupied`: slots in use.
-std::vector<std::shared_ptr<Request>> select_admissions(vfd_server *s, int occupied, size_t used)
+// larger than the whole budget is rejected).  A request that fits only once
+// pooled worlds are freed gets them freed first (the pool's bytes count
+// against the budget; a pooled world of its own shape is reused instead).
+std::vector<std::shared_ptr<Request>> select_admissions(vfd_server *s, int occupied)
 {
     std::vector<std::shared_ptr<Request>> out;
+    std::map<std::string, size_t> taken;  // pooled worlds already promised, by key
     std::unique_lock<std::mutex> lk(s->mu);
     int slots = s->max_active - occupied;
+    size_t used = s->in_use;
     while (!s->pending.empty() && slots > 0) {
         auto r = s->pending.front();
         const size_t est = estimate_bytes(*r);
@@ -213,8 +325,20 @@ std::vector<std::shared_ptr<Request>> select_admissions(vfd_server *s, int occup
             lk.lock();
             continue;
         }
-        if (used + est > s->budget) break;  // FIFO: wait for memory
-        used += est;
+        const std::string key = world_key(*r);
+        bool pooled = s->pool.count(key) > taken[key];
+        if (!pooled && used + est > s->budget) {
+            if (s->pool_bytes == 0) break;  // FIFO: wait for memory
+            lk.unlock();
+            free_idle(s);  // device idle: pooled worlds are freed
+            lk.lock();
+            taken.clear();
+            used = s->in_use;
+            for (auto &q : out) used += estimate_bytes(*q);
+            if (used + est > s->budget) break;
+        }
+        if (pooled) taken[key]++;
+        else used += est;
         out.push_back(r);
         s->pending.pop_front();
         --slots;
@@ -223,19 +347,20 @@ std::vector<std::shared_ptr<Request>> select_admissions(vfd_server *s, int occup
     return out;
 }
 
-// Creates the worlds of selected requests; returns those that are resident.
+// Creates (or reuses) the worlds of selected requests; returns those that are resident.
 std::vector<std::shared_ptr<Request>> admit_all(vfd_server *s, const std::vector<std::shared_ptr<Request>> &sel)
 {
     std::vector<std::shared_ptr<Request>> ok;
     for (auto &r : sel) {
         std::string msg;
+        bool reused = false;
         r->info.t_admit = s->now();
-        const int st = admit(s, r, msg);
+        const int st = admit(s, r, &reused, msg);
         if (st != VFD_OK) {
             finish(s, r, st, msg);
             continue;
         }
-        s->in_use += r->bytes;
+        if (!reused) s->in_use += r->bytes;
         ok.push_back(r);
         std::lock_guard<std::mutex> lk(s->mu);
         s->st.admitted++;
@@ -243,46 +368,53 @@ std::vector<std::shared_ptr<Request>> admit_all(vfd_server *s, const std::vector
     return ok;
 }
 
-// The scheduler overlaps host work with the device: while a round runs, the
-// requests that finish with it are already known, so new requests are
-// admitted and the next round's batch is built before the round ends; after
-// it ends the finished requests are retired and the next round starts at once.
+void note_busy(vfd_server *s, bool busy)
+{
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (busy && s->busy_since < 0) s->busy_since = s->now();
+    if (!busy && s->busy_since >= 0) {
+        s->st.busy_s += s->now() - s->busy_since;
+        s->busy_since = -1.0;
+    }
+}
+
 void scheduler(vfd_server *s)
 {
     cudaSetDevice(s->device);
     for (;;) {
-        // ---- admission while the device is idle ----------------------------
-        if (s->active.empty()) bury(s);
-        {
+        // ---- rounds: keep at most kRoundsInFlight queued ----------------------
+        while ((int)s->inflight.size() >= kRoundsInFlight || (s->active.empty() && !s->inflight.empty())) {
+            complete_oldest(s);
+            if (s->active.empty()) break;
+        }
+        if (s->active.empty() && s->inflight.empty()) {
+            note_busy(s, false);
             std::unique_lock<std::mutex> lk(s->mu);
-            s->cv_work.wait(lk, [&] { return s->stop || !s->pending.empty() || !s->active.empty(); });
+            if (s->pending.empty() && !s->stop) {
+                // idle: return pooled memory while waiting
+                lk.unlock();
+                free_idle(s);
+                lk.lock();
+            }
+            s->cv_work.wait(lk, [&] { return s->stop || !s->pending.empty(); });
             if (s->stop) break;
         }
         {
-            auto got = admit_all(s, select_admissions(s, (int)s->active.size(), s->in_use));
+            auto got = admit_all(s, select_admissions(s, (int)s->active.size()));
             if (!got.empty()) s->set_changed = true;
             s->active.insert(s->active.end(), got.begin(), got.end());
         }
-        if (s->active.empty()) {
-            bury(s);
-            std::lock_guard<std::mutex> lk(s->mu);
-            if (s->busy_since >= 0) {
-                s->st.busy_s += s->now() - s->busy_since;
-                s->busy_since = -1.0;
-            }
-            continue;
-        }
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            if (s->busy_since < 0) s->busy_since = s->now();
-        }
+        if (s->active.empty()) continue;
+        note_busy(s, true);
         if (s->set_changed || !s->batch) {
-            if (s->batch) vfd_batch_destroy(s->batch);
+            // the old batch may still be used by rounds in flight: destroyed while idle
+            if (s->batch) s->dead_batches.push_back(s->batch);
             s->batch = nullptr;
             std::vector<vfd_world *> ws;
             for (auto &r : s->active) ws.push_back(r->world);
             if (vfd_batch_create(ws.data(), (int)ws.size(), &s->batch) != VFD_OK) {
                 const std::string msg = vfd_batch_last_error(nullptr);
+                complete_all(s);
                 for (auto &r : s->active) {
                     vfd_world_destroy(r->world);
                     r->world = nullptr;
@@ -290,86 +422,62 @@ void scheduler(vfd_server *s)
                     finish(s, r, VFD_ERR_CUDA, msg);
                 }
                 s->active.clear();
+                s->batch = nullptr;
                 continue;
             }
             s->set_changed = false;
         }
 
-        // ---- one round: every active request advances one tick -----------
-        cudaEventRecord(s->ev_round[0], s->stream);
-        vfd_status st = vfd_batch_tick(s->batch, s->substeps, s->stream);
-        cudaEventRecord(s->ev_round[1], s->stream);
-
-        // while it runs: admit into the slots of requests finishing now and
-        // build the next round's batch
-        std::vector<std::shared_ptr<Request>> survivors, joining;
-        vfd_batch *next = nullptr;
-        bool next_changed = false;
-        if (st == VFD_OK) {
-            for (auto &r : s->active)
-                if (r->ticks_done + 1 < r->ticks) survivors.push_back(r);
-            joining = admit_all(s, select_admissions(s, (int)survivors.size(), s->in_use));
-            next_changed = survivors.size() != s->active.size() || !joining.empty();
-            if (next_changed && survivors.size() + joining.size() > 0) {
-                std::vector<vfd_world *> ws;
-                for (auto &r : survivors) ws.push_back(r->world);
-                for (auto &r : joining) ws.push_back(r->world);
-                if (vfd_batch_create(ws.data(), (int)ws.size(), &next) != VFD_OK) next = nullptr;  // rebuilt later
-            }
-        }
-        bury(s);  // last round's retired worlds (waits for the device)
-        if (st == VFD_OK && cudaStreamSynchronize(s->stream) != cudaSuccess) st = VFD_ERR_CUDA;
-        float round_ms = 0.0f;
-        if (st == VFD_OK) cudaEventElapsedTime(&round_ms, s->ev_round[0], s->ev_round[1]);
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            s->st.rounds++;
-            s->st.device_s += 1e-3 * round_ms;
-        }
+        // ---- launch one round: every active request advances one tick ------
+        Round rd;
+        rd.start = take_event(s);
+        rd.end = take_event(s);
+        cudaEventRecord(rd.start, s->stream);
+        const vfd_status st = vfd_batch_tick(s->batch, s->substeps, s->stream);
+        cudaEventRecord(rd.end, s->stream);
         if (st != VFD_OK) {
             const std::string msg = vfd_batch_last_error(s->batch);
+            s->inflight.push_back(std::move(rd));
+            complete_all(s);
             for (auto &r : s->active) {
                 vfd_world_destroy(r->world);
                 r->world = nullptr;
                 s->in_use -= r->bytes;
                 finish(s, r, st, msg);
             }
-            if (next) vfd_batch_destroy(next);
-            vfd_batch_destroy(s->batch);
+            s->active.clear();
+            s->dead_batches.push_back(s->batch);
             s->batch = nullptr;
-            s->active = joining;  // admitted during the failed round: not part of it
             s->set_changed = true;
-        } else {
-            for (auto &r : s->active) {
-                r->ticks_done++;
-                if (r->ticks_done >= r->ticks) {
-                    std::string msg;
-                    const int rs = retire(s, r, msg);
-                    finish(s, r, rs, msg);
-                }
-            }
-            if (next_changed) {
-                vfd_batch_destroy(s->batch);
-                s->batch = next;
-                s->set_changed = next == nullptr;
-                survivors.insert(survivors.end(), joining.begin(), joining.end());
-                s->active.swap(survivors);
-            }
+            continue;
         }
+        std::vector<std::shared_ptr<Request>> survivors;
+        for (auto &r : s->active) {
+            if (++r->ticks_launched >= r->ticks) rd.finishing.push_back(r);
+            else survivors.push_back(r);
+        }
+        if (!rd.finishing.empty()) {
+            s->active.swap(survivors);
+            s->set_changed = true;
+        }
+        s->inflight.push_back(std::move(rd));
         std::lock_guard<std::mutex> lk(s->mu);
         s->st.active = (int64_t)s->active.size();
         s->st.hbm_in_use = s->in_use;
         s->st.hbm_peak = std::max(s->st.hbm_peak, s->in_use);
     }
-    // shutdown: drop what is still resident
-    if (s->batch) vfd_batch_destroy(s->batch);
-    s->batch = nullptr;
-    bury(s);
+    // shutdown: finish the rounds in flight, drop what is still resident
+    complete_all(s);
     for (auto &r : s->active) {
         vfd_world_destroy(r->world);
         r->world = nullptr;
     }
     s->active.clear();
+    if (s->batch) s->dead_batches.push_back(s->batch);
+    s->batch = nullptr;
+    free_idle(s);
+    for (auto e : s->ev_pool) cudaEventDestroy(e);
+    s->ev_pool.clear();
 }
 
 }  // namespace
@@ -394,12 +502,10 @@ vfd_status vfd_server_create(int device, size_t hbm_budget_bytes, int max_active
     cudaGetDevice(&prev);
     cudaSetDevice(device);
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_round[0]);
-    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_round[1]);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->rstream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
-        for (auto &ev : s->ev_round)
-            if (ev) cudaEventDestroy(ev);
         if (s->stream) cudaStreamDestroy(s->stream);
+        if (s->rstream) cudaStreamDestroy(s->rstream);
         cudaSetDevice(prev);
         delete s;
         return VFD_ERR_CUDA;
@@ -449,6 +555,7 @@ vfd_status vfd_server_submit(vfd_server *s, const vfd_request_desc *d, uint64_t 
         r->info.id = r->id;
         r->info.t_submit = s->now();
         r->info.status = -1;
+        s->open_submit[r->id] = r->info.t_submit;
         s->pending.push_back(r);
         s->st.submitted++;
         s->st.queued = (int64_t)s->pending.size();
@@ -495,12 +602,19 @@ vfd_status vfd_server_get_stats(vfd_server *s, vfd_server_stats *out)
     if (!s || !out) return VFD_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(s->mu);
     *out = s->st;
-    if (s->busy_since >= 0) out->busy_s += s->now() - s->busy_since;
-    out->p50_latency_s = percentile(s->latencies, 0.50);
-    out->p99_latency_s = percentile(s->latencies, 0.99);
+    const double t = s->now();
+    if (s->busy_since >= 0) out->busy_s += t - s->busy_since;
+    out->p50_completed_s = percentile(s->latencies, 0.50);
+    out->p99_completed_s = percentile(s->latencies, 0.99);
+    // every arrival: the unfinished ones with the time they have waited so far
+    std::vector<double> all(s->latencies);
+    for (const auto &kv : s->open_submit) all.push_back(t - kv.second);
+    out->censored = (int64_t)s->open_submit.size();
+    out->p50_latency_s = percentile(all, 0.50);
+    out->p99_latency_s = percentile(all, 0.99);
     double m = 0.0;
-    for (double x : s->latencies) m += x;
-    out->mean_latency_s = s->latencies.empty() ? 0.0 : m / (double)s->latencies.size();
+    for (double x : all) m += x;
+    out->mean_latency_s = all.empty() ? 0.0 : m / (double)all.size();
     return VFD_OK;
 }
 
@@ -518,8 +632,8 @@ vfd_status vfd_server_destroy(vfd_server *s)
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(s->device);
-    for (auto &ev : s->ev_round) cudaEventDestroy(ev);
     cudaStreamDestroy(s->stream);
+    cudaStreamDestroy(s->rstream);
     cudaSetDevice(prev);
     delete s;
     return VFD_OK;

@@ -1897,6 +1897,9 @@ struct vfd_batch {
     uint64_t graph_launches = 0;
     int same_ticks = 0;  // ticks in a row with the current substep count and sources
     std::vector<uint64_t> gens;
+    std::vector<OsJob> oj;       // host copy of the overlap-save jobs ([axis][njobs])
+    bool can_os[3] = {false, false, false};
+    float tuned_ms[3] = {0.0f, 0.0f, 0.0f};
     std::string err;
 };
 
@@ -2004,6 +2007,7 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
             for (int f = 0; f < w->nf; ++f) rmn = std::min(rmn, w->params[f].radius[a]);
         }
         b->use_os[a] = all;
+        b->can_os[a] = all;
         b->rmin[a] = rmn;
         b->os_minb[a] = b->worlds[0]->os_minb[a];
         for (auto *w : b->worlds)
@@ -2049,8 +2053,125 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
         return bfail(nullptr, e == cudaErrorMemoryAllocation ? VFD_ERR_OUT_OF_MEMORY : VFD_ERR_CUDA, msg);
     }
     b->gens.assign(n_worlds, ~0ull);
+    b->oj.swap(oj);
     *out = b;
     return VFD_OK;
+}
+
+// Times one axis pass of the whole batch as configured now (one warm-up,
+// `reps` timed launches, CUDA events on the batch stream).
+static vfd_status batch_time_axis(vfd_batch *b, int a, int reps, cudaEvent_t e0, cudaEvent_t e1, float *ms)
+{
+    for (int it = -1; it < reps; ++it) {
+        if (it == 0) VFD_BCUDA(b, cudaEventRecord(e0, b->st));
+        if (b->use_rf[a])
+            VFD_BCUDA(b, launch_rf_groups(b->d_osjobs + a * b->njobs, b->rf[a], a, b->st));
+        else if (b->use_os[a])
+            VFD_BCUDA(b, launch_os(b->d_osjobs + a * b->njobs, b->d_os_tiles[a], b->os_tiles[a], b->rmin[a], a, b->st,
+                                   b->os_minb[a]));
+        else
+            VFD_BCUDA(b, launch_axis(b->variant[a], b->d_jobs + a * b->njobs, b->njobs, b->tiles[a], b->Fmax[a],
+                                     b->st));
+    }
+    VFD_BCUDA(b, cudaEventRecord(e1, b->st));
+    VFD_BCUDA(b, cudaEventSynchronize(e1));
+    VFD_BCUDA(b, cudaEventElapsedTime(ms, e0, e1));
+    *ms /= (float)reps;
+    return VFD_OK;
+}
+
+vfd_status vfd_batch_autotune(vfd_batch *b, int reps, vfd_axis_tuning *out3)
+{
+    if (!b) return VFD_ERR_INVALID_ARG;
+    if (reps < 1) reps = 3;
+    DeviceGuard g(b->device);
+    VFD_BCUDA(b, cudaStreamSynchronize(b->st));
+    // the passes run on the worlds' own fields: save them, restore after
+    std::vector<float *> saved(b->worlds.size(), nullptr);
+    auto restore = [&](bool copy) {
+        for (size_t i = 0; i < b->worlds.size(); ++i) {
+            vfd_world *w = b->worlds[i];
+            if (copy && saved[i])
+                cudaMemcpyAsync(w->d_fields, saved[i], sizeof(float) * w->V * w->nf, cudaMemcpyDeviceToDevice, b->st);
+        }
+        cudaStreamSynchronize(b->st);
+        for (auto p : saved) cudaFree(p);
+    };
+    for (size_t i = 0; i < b->worlds.size(); ++i) {
+        vfd_world *w = b->worlds[i];
+        cudaError_t e = cudaMalloc(&saved[i], sizeof(float) * w->V * w->nf);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(saved[i], w->d_fields, sizeof(float) * w->V * w->nf, cudaMemcpyDeviceToDevice, b->st);
+        if (e != cudaSuccess) {
+            restore(false);
+            return bfail(b, e == cudaErrorMemoryAllocation ? VFD_ERR_OUT_OF_MEMORY : VFD_ERR_CUDA,
+                         std::string("autotune backup: ") + cudaGetErrorString(e));
+        }
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    vfd_status st = VFD_OK;
+    for (int a = 0; a < 3 && st == VFD_OK; ++a) {
+        // register-FFT groups for this axis if every job allows them
+        bool rf_ok = !b->rf[a].empty();
+        if (!rf_ok && b->can_os[a] && rf_enabled() && !b->oj.empty()) {
+            bool ok = true;
+            for (int i = 0; i < b->njobs; ++i) ok = ok && rf_eligible(b->oj[(size_t)a * b->njobs + i]);
+            if (ok && rf_prepare() == cudaSuccess &&
+                build_rf_groups(&b->oj[(size_t)a * b->njobs], b->njobs, b->rf[a]) == cudaSuccess)
+                rf_ok = !b->rf[a].empty();
+        }
+        struct Cand {
+            int method, minb;
+        };
+        std::vector<Cand> cands;
+        if (rf_ok) cands.push_back({PASS_METHOD_RF, 0});
+        if (b->can_os[a]) {
+            cands.push_back({PASS_METHOD_OS, 3});
+            cands.push_back({PASS_METHOD_OS, 4});
+        }
+        cands.push_back({PASS_METHOD_FULL, 0});
+        float best = 0.0f;
+        Cand bc = cands.back();
+        for (const Cand &c : cands) {
+            b->use_rf[a] = c.method == PASS_METHOD_RF;
+            b->use_os[a] = c.method == PASS_METHOD_OS;
+            b->os_minb[a] = c.minb;
+            float ms = 0.0f;
+            st = batch_time_axis(b, a, reps, e0, e1, &ms);
+            if (st != VFD_OK) break;
+            if (best == 0.0f || ms < best) {
+                best = ms;
+                bc = c;
+            }
+        }
+        b->use_rf[a] = bc.method == PASS_METHOD_RF;
+        b->use_os[a] = bc.method == PASS_METHOD_OS;
+        b->os_minb[a] = bc.minb;
+        b->tuned_ms[a] = best;
+        if (out3) {
+            out3[a].method = bc.method == PASS_METHOD_RF ? VFD_PASS_REGISTER_FFT
+                             : bc.method == PASS_METHOD_OS ? VFD_PASS_OVERLAP_SAVE
+                                                           : VFD_PASS_FULL_LINE;
+            out3[a].ctas_per_sm = bc.minb;
+            out3[a].fft_len = bc.method == PASS_METHOD_FULL ? b->Fmax[a] : 64;
+            out3[a].radix_order = 0;
+            out3[a].variant = bc.method == PASS_METHOD_FULL ? b->variant[a] : -1;
+            out3[a].ms = best;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    restore(true);
+    // the next tick runs directly and re-captures its graph with the chosen passes
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->graph_substeps = -1;
+    b->same_ticks = 0;
+    return st;
 }
 
 vfd_status vfd_batch_destroy(vfd_batch *b)

@@ -46,6 +46,7 @@ EXPORTED = [
     "vfd_fft_diffuse3d_noalloc", "vfd_update_gradients", "vfd_sample_field", "vfd_write_vtk",
     "vfd_autotune", "vfd_world_tuning", "vfd_autotune_set", "vfd_autotune_clear",
     "vfd_set_spectrum", "vfd_set_boundary", "vfd_tick_update", "vfd_diffuse_update_host",
+    "vfd_batch_autotune",
 ]
 
 PASS_METHODS = {0: "register_fft", 1: "overlap_save", 2: "full_line"}
@@ -101,7 +102,8 @@ class ServerStats(C.Structure):
                 ("rounds", C.c_int64), ("busy_s", C.c_double), ("voxel_steps_done", C.c_double),
                 ("p50_latency_s", C.c_double), ("p99_latency_s", C.c_double),
                 ("mean_latency_s", C.c_double), ("hbm_in_use", C.c_size_t), ("hbm_peak", C.c_size_t),
-                ("device_s", C.c_double)]
+                ("device_s", C.c_double), ("p50_completed_s", C.c_double), ("p99_completed_s", C.c_double),
+                ("censored", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -143,6 +145,7 @@ def load(path=LIB_PATH):
     lib.vfd_diffuse_update_host.argtypes = [P, C.POINTER(P), C.POINTER(P), P, C.c_int]
     lib.vfd_batch_create.argtypes = [C.POINTER(P), C.c_int, C.POINTER(P)]
     lib.vfd_batch_tick.argtypes = [P, C.c_int, P]
+    lib.vfd_batch_autotune.argtypes = [P, C.c_int, P]
     lib.vfd_batch_destroy.argtypes = [P]
     lib.vfd_batch_last_error.argtypes = [P]
     lib.vfd_batch_last_error.restype = C.c_char_p
@@ -442,6 +445,15 @@ class Batch:
         st = lib().vfd_batch_tick(self._h, n_substeps, stream)
         if st != 0:
             raise VfdError(st, lib().vfd_batch_last_error(self._h).decode())
+
+    def autotune(self, reps=3):
+        """Times each axis pass candidate over the whole batch and keeps the
+        fastest; returns one dict per axis (x, y, z)."""
+        out = (AxisTuning * 3)()
+        st = lib().vfd_batch_autotune(self._h, int(reps), out)
+        if st != 0:
+            raise VfdError(st, lib().vfd_batch_last_error(self._h).decode())
+        return [out[a].as_dict() for a in range(3)]
 
     def close(self):
         if getattr(self, "_h", None):
