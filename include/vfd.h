@@ -205,6 +205,15 @@ vfd_status vfd_set_window(vfd_world *w, int field, const float *window, int kw, 
  * VFD_METHOD_PLAIN only (VFD_ERR_NOT_SUPPORTED otherwise). */
 vfd_status vfd_set_spectrum(vfd_world *w, int field, const float *kspec, int fx, int fy, int fz);
 
+/* computeKernelSpectrum3D (Diffusion.cu:1533-1619) without cuFFT: the
+ * unscaled R2C spectrum of the window (kd*kh*kw, x fastest) wrapped with its
+ * centre (cx, cy, cz) at index 0 (padKernel3D, convolutionFFT.cuh:402-445) on
+ * the fx*fy*fz grid, computed on `device` with this library's FFT and written
+ * to out (host, fz*fy*(fx/2+1) interleaved (re, im) floats: the layout of
+ * chem_cctx->h_kernelspectrum[ic]).  fx even, 7-smooth lengths. */
+vfd_status vfd_window_spectrum(const float *window, int kw, int kh, int kd, int cx, int cy, int cz,
+                               int fx, int fy, int fz, float *out, int device);
+
 /* Changes the constant-VF padding of a VFD_METHOD_FFT3D / VFD_METHOD_PLAIN
  * world between ticks: the x bound (the reference passes rightWallIndex =
  * bmcx - 1 to every diffuseChemGPU call, woundHealingWorld.cpp:2407) and,

@@ -42,6 +42,8 @@ def lib():
         L.vfo_conv_clamp2d.argtypes = [C.c_int, C.c_int, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P]
         L.vfo_stencil_power.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, _P]
         L.vfo_stencil_power.restype = C.c_int
+        L.vfo_stencil_power_spectral.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _P]
+        L.vfo_stencil_power_spectral.restype = C.c_int
         L.vfo_substep.argtypes = ([C.c_int] * 3 + [_P, _P] + [C.c_double] * 3 + [C.c_int] * 3 +
                                   [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int] +
                                   [C.c_int] * 3 + [_P])
@@ -197,6 +199,27 @@ def stencil_power(lam, gamma_dt, n_steps, R):
     w = np.empty((2 * R + 1,) * 3, np.float64)
     assert lib().vfo_stencil_power(float(lam), float(gamma_dt), int(n_steps), int(R), _p(w)) == 0
     return w
+
+
+def stencil_power_spectral(lam, gamma_dt, n_steps, R, G):
+    """The same window from the stencil's spectrum on a periodic G^3 grid (FP64)."""
+    w = np.empty((2 * R + 1,) * 3, np.float64)
+    assert lib().vfo_stencil_power_spectral(float(lam), float(gamma_dt), int(n_steps), int(R), int(G), _p(w)) == 0
+    return w
+
+
+def ref_compute_kernel3d(lam, gamma_dt, kernel_radius, niter, F, window):
+    """The reference's computeKernel3D (its own kernels + cuFFT, GPU)."""
+    L = C.CDLL(REF_REPLAY)
+    f = L.ref_compute_kernel3d
+    f.argtypes = [C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, _P]
+    f.restype = C.c_int
+    L.ref_replay_error.restype = C.c_char_p
+    out = np.empty((window,) * 3, np.float32)
+    rc = f(float(lam), float(gamma_dt), int(kernel_radius), int(niter), int(F), int(window), _p(out))
+    if rc != 0:
+        raise RuntimeError("ref computeKernel3D replay failed: " + L.ref_replay_error().decode())
+    return out
 
 
 def update(t, d, decay):

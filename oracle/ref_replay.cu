@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 #include <cufft.h>
 #include <stdio.h>
+#include <stdlib.h>
 
 extern "C" void padKernel3D(float *d_Dst, float *d_Src, int fftD, int fftH, int fftW, int kernelD,
                             int kernelH, int kernelW, int kernelZ, int kernelY, int kernelX);
@@ -22,6 +23,12 @@ extern "C" void modulateAndNormalize3D(float2 *d_Dst, float2 *d_Src, int fftD, i
                                        int padding);
 extern "C" void unpadResult3D(float *d_Dst, float *d_Src, int dataD, int dataH, int dataW, int fftD,
                               int fftH, int fftW);
+extern "C" void padDataClampToBorder3D(float *d_Dst, float *d_Src, int fftD, int fftH, int fftW, int dataD,
+                                       int dataH, int dataW, int kernelD, int kernelH, int kernelW, int kernelZ,
+                                       int kernelY, int kernelX);
+extern "C" void complexPower(float2 *d_Dst, int fftD, int fftH, int fftW, int padding, int n);
+extern "C" void extractCenter3D(float *d_Dst, float *d_Src, int dataD, int dataH, int dataW, int windowD,
+                                int windowH, int windowW);
 
 #define RR_CHECK(x)                                                                    \
     do {                                                                               \
@@ -132,6 +139,88 @@ done:
     cudaFree(d_win);
     cudaFree(d_pk);
     cudaFree(d_ks);
+    return rc;
+}
+
+// computeKernel3D (Diffusion.cu:1078-1401) replayed with the reference's own
+// kernels and cuFFT: the 3x3x3 stencil (centre 1 - 6 lambda - gamma_dt, six
+// arms lambda) placed at the centre of a D^3 data cube (D = 2 (kernelRadius -
+// 1) + 1); niter rounds of padKernel3D(stencil) + padDataClampToBorder3D(data)
+// on the F^3 grid, R2C of both, complexPower(K, kernelRadius - 1 - [first
+// round]), modulateAndNormalize3D, C2R, unpadResult3D; then the centred
+// window^3 (extractCenter3D) into h_window.  The reference's human-VF setting
+// is kernelRadius 150, niter 6, F 616, window 147 (DiffusionHelper.cpp:48-100).
+extern "C" int ref_compute_kernel3d(float lambda, float gamma_dt, int kernelRadius, int niter, int F, int window,
+                                    float *h_window)
+{
+    int rc = 0;
+    const int D = (kernelRadius - 1) * 2 + 1;
+    const size_t dsz = (size_t)D * D * D, fsz = (size_t)F * F * F, ssz = (size_t)F * F * (F / 2 + 1);
+    const size_t wsz = (size_t)window * window * window;
+    float *d_data = nullptr, *d_kern = nullptr, *d_pdata = nullptr, *d_pkern = nullptr, *d_win = nullptr;
+    float2 *d_kspec = nullptr, *d_dspec = nullptr;
+    float *h_data = nullptr;
+    cufftHandle fwd = 0, inv = 0;
+    bool have_fwd = false, have_inv = false;
+    float h_kern[27];
+    for (int i = 0; i < 27; ++i) h_kern[i] = 0.0f;
+    // Diffusion.cu:1182-1195: z-arms, y-arms, x-arms and the centre
+    h_kern[0 * 9 + 1 * 3 + 1] = lambda;
+    h_kern[2 * 9 + 1 * 3 + 1] = lambda;
+    h_kern[1 * 9 + 0 * 3 + 1] = lambda;
+    h_kern[1 * 9 + 2 * 3 + 1] = lambda;
+    h_kern[1 * 9 + 1 * 3 + 0] = lambda;
+    h_kern[1 * 9 + 1 * 3 + 2] = lambda;
+    h_kern[1 * 9 + 1 * 3 + 1] = 1.0f - 6.0f * lambda - gamma_dt;
+    h_data = (float *)calloc(dsz, sizeof(float));
+    if (!h_data) return -3;
+    // the stencil at the centre of the data cube (Diffusion.cu:1207-1226)
+    for (int k = 0; k < 3; ++k)
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                h_data[((size_t)(D / 2 - 1 + k) * D + (D / 2 - 1 + i)) * D + (D / 2 - 1 + j)] = h_kern[k * 9 + i * 3 + j];
+    RR_CHECK(cudaMalloc(&d_data, dsz * sizeof(float)));
+    RR_CHECK(cudaMalloc(&d_kern, 27 * sizeof(float)));
+    RR_CHECK(cudaMalloc(&d_pdata, fsz * sizeof(float)));
+    RR_CHECK(cudaMalloc(&d_pkern, fsz * sizeof(float)));
+    RR_CHECK(cudaMalloc(&d_kspec, ssz * sizeof(float2)));
+    RR_CHECK(cudaMalloc(&d_dspec, ssz * sizeof(float2)));
+    RR_CHECK(cudaMalloc(&d_win, wsz * sizeof(float)));
+    RR_CHECK(cudaMemcpy(d_kern, h_kern, 27 * sizeof(float), cudaMemcpyHostToDevice));
+    RR_CHECK(cudaMemcpy(d_data, h_data, dsz * sizeof(float), cudaMemcpyHostToDevice));
+    RR_CHECK(cudaMemset(d_pkern, 0, fsz * sizeof(float)));
+    RR_CHECK(cudaMemset(d_pdata, 0, fsz * sizeof(float)));
+    RR_CUFFT(cufftPlan3d(&fwd, F, F, F, CUFFT_R2C));
+    have_fwd = true;
+    RR_CUFFT(cufftPlan3d(&inv, F, F, F, CUFFT_C2R));
+    have_inv = true;
+    for (int it = 0; it < niter; ++it) {
+        padKernel3D(d_pkern, d_kern, F, F, F, 3, 3, 3, 1, 1, 1);
+        padDataClampToBorder3D(d_pdata, d_data, F, F, F, D, D, D, 3, 3, 3, 1, 1, 1);
+        RR_CHECK(cudaGetLastError());
+        RR_CUFFT(cufftExecR2C(fwd, (cufftReal *)d_pkern, (cufftComplex *)d_kspec));
+        RR_CUFFT(cufftExecR2C(fwd, (cufftReal *)d_pdata, (cufftComplex *)d_dspec));
+        complexPower(d_kspec, F, F, F, 1, kernelRadius - (it == 0 ? 1 : 0) - 1);
+        modulateAndNormalize3D(d_dspec, d_kspec, F, F, F, 1);
+        RR_CHECK(cudaGetLastError());
+        RR_CUFFT(cufftExecC2R(inv, (cufftComplex *)d_dspec, (cufftReal *)d_pdata));
+        unpadResult3D(d_data, d_pdata, D, D, D, F, F, F);
+        RR_CHECK(cudaGetLastError());
+    }
+    extractCenter3D(d_win, d_data, D, D, D, window, window, window);
+    RR_CHECK(cudaGetLastError());
+    RR_CHECK(cudaMemcpy(h_window, d_win, wsz * sizeof(float), cudaMemcpyDeviceToHost));
+done:
+    if (have_fwd) cufftDestroy(fwd);
+    if (have_inv) cufftDestroy(inv);
+    cudaFree(d_data);
+    cudaFree(d_kern);
+    cudaFree(d_pdata);
+    cudaFree(d_pkern);
+    cudaFree(d_kspec);
+    cudaFree(d_dspec);
+    cudaFree(d_win);
+    free(h_data);
     return rc;
 }
 

@@ -50,7 +50,7 @@ using Diffuser = vfd::DiffuserShim<c_ctx, ChemStandIn>;
 // WHWorld::initializeChemGPU's kernel part: returns the constructed Diffuser
 // after the kernel context has gone.
 Diffuser *init_like_reference(c_ctx *chem_cctx, ChemStandIn *chem, int nchem, const float *const *windows, int k,
-                              std::string &err)
+                              const float *lambdas, int n_steps, std::string &err)
 {
     c_ctx kernel_cctx;
     std::memset(&kernel_cctx, 0, sizeof(kernel_cctx));
@@ -59,7 +59,16 @@ Diffuser *init_like_reference(c_ctx *chem_cctx, ChemStandIn *chem, int nchem, co
     for (int ig = 0; ig < N_GPU; ++ig) kernel_cctx.h_data[ig] = (float *)std::malloc(wbytes);
     for (int ic = N_GPU; ic < N_CHEM; ++ic) kernel_cctx.h_data[ic] = kernel_cctx.h_data[ic % N_GPU];
     const int fD = chem_cctx->FFTD, fH = chem_cctx->FFTH, fW = chem_cctx->FFTW;
-    for (int ic = 0; ic < nchem; ++ic) {
+    if (lambdas) {
+        // this library's kernel preparation in place of prepKernel (no cuFFT)
+        const vfd_status s = vfd::prepKernelSpectra(chem_cctx, lambdas, nullptr, nchem, n_steps, 0);
+        if (s != VFD_OK) {
+            err = std::string("prepKernelSpectra: ") + vfd_last_error(nullptr);
+            for (int ig = 0; ig < N_GPU; ++ig) std::free(kernel_cctx.h_data[ig]);
+            return nullptr;
+        }
+    }
+    for (int ic = 0; ic < nchem && !lambdas; ++ic) {
         // computeKernel3D leaves chemical ic's window in the shared per-GPU buffer
         std::memcpy(kernel_cctx.h_data[ic], windows[ic], wbytes);
         if (ref_kernel_spectrum(kernel_cctx.h_data[ic], chem_cctx->KD, chem_cctx->KH, chem_cctx->KW, chem_cctx->KZ,
@@ -82,12 +91,16 @@ Diffuser *init_like_reference(c_ctx *chem_cctx, ChemStandIn *chem, int nchem, co
 // FFTH, FFTD; p_in[ic]: initial pChem.  decay == NULL: `calls` x
 // diffuseChemGPU(epi), out[ic] <- tChem[ic] (h_obuffs).  Otherwise `calls` x
 // diffuseAndUpdateChemGPU(epi, decay) with dChem[ic] <- d_in[ic] before each
-// call, out[ic] <- pChem[ic], totals[ic] <- total[ic].  Returns the shim's
-// status (or -1 when the harness itself failed); err receives the message.
+// call, out[ic] <- pChem[ic], totals[ic] <- total[ic].  lambdas != NULL: the
+// spectra come from vfd::prepKernelSpectra (stencil to the power n_steps,
+// this library's FFT) instead of the reference's padKernel3D + cuFFT of
+// windows[ic].  Returns the shim's status (or -1 when the harness itself
+// failed); err receives the message.
 extern "C" int shim_harness_run(int nx, int ny, int nz, int nchem, const float *const *windows, int k,
                                 const int *fft3, const float *baselines, const float *const *p_in,
                                 float *const *out, int epi, int calls, const float *decay,
-                                const float *const *d_in, float *totals, char *err, int errlen)
+                                const float *const *d_in, float *totals, const float *lambdas, int n_steps,
+                                char *err, int errlen)
 {
     if (nchem < 1 || nchem > N_CHEM || k < 1 || (k & 1) == 0) return -1;
     const size_t V = (size_t)nx * ny * nz;
@@ -123,7 +136,7 @@ extern "C" int shim_harness_run(int nx, int ny, int nz, int nchem, const float *
         chem_cctx->h_obuffs[ic] = chem.tChem[ic];
         chem_cctx->h_kernelspectrum[ic] = (fComplex *)std::malloc(nspec * sizeof(fComplex));
     }
-    Diffuser *d = init_like_reference(chem_cctx, &chem, nchem, windows, k, msg);
+    Diffuser *d = init_like_reference(chem_cctx, &chem, nchem, windows, k, lambdas, n_steps, msg);
     if (!d) {
         rc = -1;
     } else {

@@ -54,20 +54,22 @@ def _setup(nx, ny, nz, R, steps):
     return k, wins, fft, base, ins
 
 
-def _run(nx, ny, nz, wins, k, fft, base, ins, epi, calls, decay=None, dins=None):
+def _run(nx, ny, nz, wins, k, fft, base, ins, epi, calls, decay=None, dins=None, lambdas=None, n_steps=0):
     lib = C.CDLL(SHIM)
     f = lib.shim_harness_run
     P = C.c_void_p
-    f.argtypes = [C.c_int] * 4 + [P, C.c_int, P, P, P, P, C.c_int, C.c_int, P, P, P, P, C.c_int]
+    f.argtypes = [C.c_int] * 4 + [P, C.c_int, P, P, P, P, C.c_int, C.c_int, P, P, P, P, C.c_int, P, C.c_int]
     f.restype = C.c_int
     arr = lambda xs: (P * len(xs))(*[x.ctypes.data for x in xs])
     outs = [np.empty_like(u) for u in ins]
     totals = np.zeros(8, np.float32)
     err = C.create_string_buffer(512)
     fft3 = np.array(fft, np.int32)
+    lam = None if lambdas is None else np.asarray(lambdas, np.float32)
     rc = f(nx, ny, nz, 8, arr(wins), k, fft3.ctypes.data, base.ctypes.data, arr(ins), arr(outs), epi, calls,
            None if decay is None else np.asarray(decay, np.float32).ctypes.data,
-           None if dins is None else arr(dins), totals.ctypes.data, err, 512)
+           None if dins is None else arr(dins), totals.ctypes.data,
+           None if lam is None else lam.ctypes.data, n_steps, err, 512)
     assert rc == 0, err.value.decode()
     return outs, totals
 
@@ -107,3 +109,19 @@ def test_diffuser_dropin_device_update(gpu):
         assert rel_l2(outs[c], p) <= 1e-5, (c, rel_l2(outs[c], p))
         s = outs[c].astype(np.float64).sum()
         assert abs(float(totals[c]) - s) <= 1e-6 * abs(s) + 1e-30, c
+
+
+@pytest.mark.skipif(not os.path.exists(SHIM), reason="oracle/_ref/libref_shim.so not built (no reference tree)")
+def test_diffuser_dropin_with_own_kernel_preparation(gpu):
+    """vfd::prepKernelSpectra in place of the reference's prepKernel: the
+    stencil window and its spectrum computed with this library (no cuFFT);
+    each chemical's diffusion still equals the reference's kernels + cuFFT
+    fed the same stencil window (the FP64 oracle's)."""
+    nx, ny, nz, R = 40, 34, 28, 6
+    epi = 33
+    steps = 12
+    k, wins, fft, base, ins = _setup(nx, ny, nz, R, steps)
+    outs, _ = _run(nx, ny, nz, wins, k, fft, base, ins, epi, calls=1, lambdas=LAMBDAS, n_steps=steps)
+    for c in range(8):
+        ref = oracle.ref_replay(ins[c], fft, wins[c], (R, R, R), epi, float(base[c]))
+        assert rel_l2(outs[c], ref) <= 1e-5, (c, rel_l2(outs[c], ref))

@@ -245,3 +245,30 @@ def test_tick_update_against_oracle(gpu, method):
         assert float(dev_d[f].abs().max()) == 0.0
         s = outs[f].astype(np.float64).sum()
         assert abs(mass[f]["total"] - s) <= 1e-6 * s
+
+
+@pytest.mark.parametrize("lam", [0.1333, 0.0667])
+def test_stencil_window_at_reference_size(gpu, lam):
+    """The reference's human-VF kernel: the 7-point stencil to the power 894
+    (niter 6 x (kernelRadius 150 - 1), DiffusionHelper.cpp:48-100), window
+    147^3 (R = 73).  vfd_stencil_window against the FP64 spectral oracle, and
+    -- when oracle/_ref is built -- against the reference's own
+    computeKernel3D (its padKernel3D / padDataClampToBorder3D / complexPower /
+    modulateAndNormalize3D / unpadResult3D / extractCenter3D kernels + cuFFT on
+    the 616^3 grid, Diffusion.cu:1078-1401); every window passes the
+    reference's own normalisation check |sum - 1| <= 1e-3 (Diffusion.cu:1449-1454)."""
+    R, n = 73, 894
+    got = vfd.stencil_window(lam, 0.0, n, R)
+    ref64 = oracle.stencil_power_spectral(lam, 0.0, n, R, 256)
+    e64 = rel_l2(got, ref64)
+    print(f"lambda {lam}: vfd vs FP64 rel_l2 {e64:.3e}, sum {got.astype(np.float64).sum():.8f}")
+    assert e64 <= REL_L2
+    assert abs(float(got.astype(np.float64).sum()) - 1.0) <= 1e-3
+    if oracle.ref_replay_available():
+        refw = oracle.ref_compute_kernel3d(lam, 0.0, 150, 6, 616, 2 * R + 1)
+        er = rel_l2(got, refw)
+        er64 = rel_l2(refw, ref64)
+        print(f"lambda {lam}: vfd vs reference rel_l2 {er:.3e}, reference vs FP64 {er64:.3e}, "
+              f"reference sum {refw.astype(np.float64).sum():.8f}")
+        assert abs(float(refw.astype(np.float64).sum()) - 1.0) <= 1e-3
+        assert er <= REL_L2 and er64 <= REL_L2

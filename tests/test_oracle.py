@@ -234,3 +234,13 @@ def test_multithreaded_oracle_equals_serial_oracle():
         b, lk = oracle.tick_mt(u, sig, 0.05, 3, idx, amt)
         assert float(np.abs(a - b).max()) <= 1e-15 * float(np.abs(a).max())
         assert lk.shape == (3,)
+
+
+@pytest.mark.parametrize("lam,n,R,G", [(0.1333, 30, 12, 96), (0.0667, 60, 14, 80), (0.1, 7, 9, 32)])
+def test_spectral_stencil_oracle_equals_explicit_iteration(lam, n, R, G):
+    """The FP64 spectral form of the stencil power (used at the reference's
+    894-step size, where explicit iteration is out of reach) equals the
+    explicit 7-point iteration."""
+    a = oracle.stencil_power(lam, 0.0, n, R)
+    b = oracle.stencil_power_spectral(lam, 0.0, n, R, G)
+    assert float(np.abs(a - b).max()) <= 1e-14 * float(a.max())

@@ -1082,6 +1082,54 @@ vfd_status vfd_set_window(vfd_world *w, int field, const float *window, int kw, 
     return VFD_OK;
 }
 
+vfd_status vfd_window_spectrum(const float *window, int kw, int kh, int kd, int cx, int cy, int cz, int fx, int fy,
+                               int fz, float *out, int device)
+{
+    if (!window || !out || kw < 1 || kh < 1 || kd < 1 || cx < 0 || cx >= kw || cy < 0 || cy >= kh || cz < 0 ||
+        cz >= kd)
+        return fail(nullptr, VFD_ERR_INVALID_ARG, "bad window, centre or output");
+    const int rx = std::max(1, std::max(cx, kw - 1 - cx)), ry = std::max(1, std::max(cy, kh - 1 - cy)),
+              rz = std::max(1, std::max(cz, kd - 1 - cz));
+    if (fx - rx < 1 || fy - ry < 1 || fz - rz < 1 || (fx & 1))
+        return fail(nullptr, VFD_ERR_INVALID_ARG, "FFT grid smaller than the window (or odd x length)");
+    // a one-field world whose FFT grid is (fx, fy, fz): its set-up computes the
+    // spectrum with this library's transform
+    vfd_field_params p;
+    memset(&p, 0, sizeof(p));
+    p.sigma[0] = p.sigma[1] = p.sigma[2] = 1.0;
+    p.radius[0] = rx;
+    p.radius[1] = ry;
+    p.radius[2] = rz;
+    vfd_world_desc d;
+    memset(&d, 0, sizeof(d));
+    d.nx = fx - rx;
+    d.ny = fy - ry;
+    d.nz = fz - rz;
+    d.n_fields = 1;
+    d.fields = &p;
+    d.fft[0] = fx;
+    d.fft[1] = fy;
+    d.fft[2] = fz;
+    d.method = VFD_METHOD_FFT3D;
+    vfd_world *w = nullptr;
+    vfd_status st = vfd_world_create(&d, device, &w);
+    if (st != VFD_OK) return st;
+    st = vfd_set_window(w, 0, window, kw, kh, kd, cx, cy, cz);
+    if (st == VFD_OK) {
+        DeviceGuard g(w->device);
+        const int64_t nk = (int64_t)w->Fxh * fy * fz;
+        cudaError_t e = cudaMemcpy(out, w->d_kspec, sizeof(float2) * nk, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            g_thread_error = std::string("window spectrum: ") + cudaGetErrorString(e);
+            st = VFD_ERR_CUDA;
+        }
+    } else {
+        g_thread_error = w->err;
+    }
+    vfd_world_destroy(w);
+    return st;
+}
+
 vfd_status vfd_set_spectrum(vfd_world *w, int field, const float *kspec, int fx, int fy, int fz)
 {
     if (!w) return VFD_ERR_INVALID_ARG;

@@ -247,4 +247,36 @@ class DiffuserShim {
     std::string err_;
 };
 
+// cuFFT-free replacement for the reference's kernel preparation
+// (diffusion_helper::prepKernel -> computeKernel3DBatch / computeKernel3D /
+// computeKernelSpectrum3D, DiffusionHelper.cpp:695-720, Diffusion.cu:988-1619):
+// for every chemical ic, the window of the 7-point stencil (centre
+// 1 - 6 lambda - gamma_dt, arms lambda) raised to nSteps, of the chemical
+// context's window size (KW x KH x KD, centre KX, KY, KZ), computed on the
+// device (vfd_stencil_window), and its spectrum on the chemical FFT grid
+// (vfd_window_spectrum) written to chem->h_kernelspectrum[ic].  The
+// reference's human-VF setting: nSteps = niter * (kernelRadius - 1) = 894
+// (DiffusionHelper.cpp:48-100), gamma_dt = gamma[ic] * dt (0 there).  Call it
+// where WHWorld::initializeChemGPU calls prepKernel; the Diffuser is then
+// constructed as before.  Needs a cubic window (KW = KH = KD, centred).
+template <class CCtx>
+vfd_status prepKernelSpectra(CCtx *chem, const float *lambda, const float *gamma_dt, int nChem, int nSteps,
+                             int device)
+{
+    if (!chem || !lambda || nChem < 1 || nSteps < 0) return VFD_ERR_INVALID_ARG;
+    const int k = chem->KW;
+    if (k < 1 || chem->KH != k || chem->KD != k || chem->KX != k / 2 || chem->KY != k / 2 || chem->KZ != k / 2)
+        return VFD_ERR_NOT_SUPPORTED;
+    const int R = k / 2;
+    std::vector<float> win((size_t)k * k * k);
+    for (int ic = 0; ic < nChem; ++ic) {
+        vfd_status s = vfd_stencil_window(lambda[ic], gamma_dt ? gamma_dt[ic] : 0.0, nSteps, R, win.data(), device);
+        if (s != VFD_OK) return s;
+        s = vfd_window_spectrum(win.data(), k, k, k, R, R, R, chem->FFTW, chem->FFTH, chem->FFTD,
+                                reinterpret_cast<float *>(chem->h_kernelspectrum[ic]), device);
+        if (s != VFD_OK) return s;
+    }
+    return VFD_OK;
+}
+
 }  // namespace vfd

@@ -46,7 +46,7 @@ EXPORTED = [
     "vfd_fft_diffuse3d_noalloc", "vfd_update_gradients", "vfd_sample_field", "vfd_write_vtk",
     "vfd_autotune", "vfd_world_tuning", "vfd_autotune_set", "vfd_autotune_clear",
     "vfd_set_spectrum", "vfd_set_boundary", "vfd_tick_update", "vfd_diffuse_update_host",
-    "vfd_batch_autotune",
+    "vfd_batch_autotune", "vfd_window_spectrum",
 ]
 
 PASS_METHODS = {0: "register_fft", 1: "overlap_save", 2: "full_line"}
@@ -140,6 +140,7 @@ def load(path=LIB_PATH):
     lib.vfd_read_profile.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     lib.vfd_set_window.argtypes = [P, C.c_int, P] + [C.c_int] * 6
     lib.vfd_set_spectrum.argtypes = [P, C.c_int, P, C.c_int, C.c_int, C.c_int]
+    lib.vfd_window_spectrum.argtypes = [P] + [C.c_int] * 9 + [P, C.c_int]
     lib.vfd_set_boundary.argtypes = [P, C.c_int, P]
     lib.vfd_tick_update.argtypes = [P, C.c_int, C.POINTER(P), P, P]
     lib.vfd_diffuse_update_host.argtypes = [P, C.POINTER(P), C.POINTER(P), P, C.c_int]
@@ -478,6 +479,18 @@ def write_vtk(field, path):
     a = np.ascontiguousarray(field, np.float32)
     nz, ny, nx = a.shape
     _check(lib().vfd_write_vtk(_ptr(a), nx, ny, nz, str(path).encode()))
+
+
+def window_spectrum(window, fft, centre=None, device=0):
+    """Unscaled R2C spectrum (complex64, (Fz, Fy, Fx/2 + 1)) of the window
+    wrapped with its centre at index 0 on the fft = (Fx, Fy, Fz) grid."""
+    w = np.ascontiguousarray(window, dtype=np.float32)
+    kd, kh, kw = w.shape
+    cz, cy, cx = centre if centre is not None else (kd // 2, kh // 2, kw // 2)
+    fx, fy, fz = fft
+    out = np.empty((fz, fy, fx // 2 + 1), np.complex64)
+    _check(lib().vfd_window_spectrum(_ptr(w), kw, kh, kd, cx, cy, cz, fx, fy, fz, _ptr(out), device))
+    return out
 
 
 def stencil_window(lam, gamma_dt, n_steps, R, device=0):
