@@ -256,7 +256,13 @@ def test_stencil_window_at_reference_size(gpu, lam):
     computeKernel3D (its padKernel3D / padDataClampToBorder3D / complexPower /
     modulateAndNormalize3D / unpadResult3D / extractCenter3D kernels + cuFFT on
     the 616^3 grid, Diffusion.cu:1078-1401); every window passes the
-    reference's own normalisation check |sum - 1| <= 1e-3 (Diffusion.cu:1449-1454)."""
+    reference's own normalisation check |sum - 1| <= 1e-3 (Diffusion.cu:1449-1454).
+    The reference's window is itself 3e-5 (relative L2) from the exact stencil
+    power: its cpow raises an FP32 spectrum to the 148th/149th power with
+    powf (Diffusion.cu:1342-1349, convolutionFFT.cuh:645-664), which
+    multiplies the FP32 rounding of each bin about 149-fold.  So this
+    library's window is held to 1e-5 against the FP64 oracle, and to the
+    reference's own distance from it (1e-4) against the reference."""
     R, n = 73, 894
     got = vfd.stencil_window(lam, 0.0, n, R)
     ref64 = oracle.stencil_power_spectral(lam, 0.0, n, R, 256)
@@ -271,4 +277,6 @@ def test_stencil_window_at_reference_size(gpu, lam):
         print(f"lambda {lam}: vfd vs reference rel_l2 {er:.3e}, reference vs FP64 {er64:.3e}, "
               f"reference sum {refw.astype(np.float64).sum():.8f}")
         assert abs(float(refw.astype(np.float64).sum()) - 1.0) <= 1e-3
-        assert er <= REL_L2 and er64 <= REL_L2
+        assert er64 <= 1e-4 and er <= 1e-4
+        # the two differ by what the reference's FP32 power adds
+        assert abs(er - er64) <= 0.1 * er64 + REL_L2
