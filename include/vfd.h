@@ -302,7 +302,7 @@ const char *vfd_batch_last_error(const vfd_batch *b);
  * request's device bytes fit hbm_budget_bytes; admitted fields stay resident
  * on the device for all the request's ticks.  Each round advances every
  * active request by one tick (substeps_per_tick substeps) with all their
- * fields in one launch per axis pass; up to three rounds are queued on the
+ * fields in one launch per axis pass; up to four rounds are queued on the
  * device at a time, so the host prepares the next rounds (admissions, batch
  * set-up) while the device works.  Finished requests are retired (totals,
  * optional download) once their last round has completed and free their

@@ -48,6 +48,9 @@ cudaError_t launch_axis(int variant, const AxisJob *jobs, int njobs, int tiles, 
 cudaError_t launch_deposit(const DepositJob *jobs, int njobs, const int32_t *idx, const float *amt,
                            int64_t total, int *err, cudaStream_t st);
 
+// Zeroes blocks[b][0 .. counts[b]) for b < n (device arrays of pointers and counts).
+cudaError_t launch_zero_blocks(double *const *blocks, const int *counts, int n, cudaStream_t st);
+
 cudaError_t launch_synth_field(uint64_t key, double lo, double span, float *out, int64_t n, cudaStream_t st);
 
 // FFT plan of length F (radices 8,7,5,4,3,2) that some kernel variant can run,

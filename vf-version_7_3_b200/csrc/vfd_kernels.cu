@@ -382,6 +382,22 @@ cudaError_t launch_axis(int variant, const AxisJob *jobs, int njobs, int tiles, 
     }
 }
 
+// Zeroes the FP64 accounting blocks of many worlds in one launch (block b:
+// blocks[b], counts[b] doubles) -- a batch's per-substep reset.
+__global__ void zero_blocks_kernel(double *const *blocks, const int *counts, int n)
+{
+    for (int b = blockIdx.x; b < n; b += gridDim.x)
+        for (int i = threadIdx.x; i < counts[b]; i += blockDim.x) blocks[b][i] = 0.0;
+}
+
+cudaError_t launch_zero_blocks(double *const *blocks, const int *counts, int n, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    zero_blocks_kernel<<<n < 1024 ? n : 1024, 64, 0, st>>>(blocks, counts, n);
+    note_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_deposit(const DepositJob *jobs, int njobs, const int32_t *idx, const float *amt,
                            int64_t total, int *err, cudaStream_t st)
 {

@@ -40,7 +40,7 @@
 
 namespace {
 
-constexpr int kRoundsInFlight = 3;
+constexpr int kRoundsInFlight = 4;
 
 struct Request {
     uint64_t id = 0;

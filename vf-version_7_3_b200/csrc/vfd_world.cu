@@ -1945,6 +1945,8 @@ struct vfd_batch {
     uint64_t graph_launches = 0;
     int same_ticks = 0;  // ticks in a row with the current substep count and sources
     std::vector<uint64_t> gens;
+    double **d_mass_ptrs = nullptr;  // every world's accounting block, zeroed per substep in one launch
+    int *d_mass_counts = nullptr;
     std::vector<OsJob> oj;       // host copy of the overlap-save jobs ([axis][njobs])
     bool can_os[3] = {false, false, false};
     float tuned_ms[3] = {0.0f, 0.0f, 0.0f};
@@ -1980,6 +1982,8 @@ static void batch_release(vfd_batch *b)
         cudaFree(b->d_os_tiles[a]);
         free_rf_groups(b->rf[a]);
     }
+    cudaFree(b->d_mass_ptrs);
+    cudaFree(b->d_mass_counts);
     if (b->ev_in) cudaEventDestroy(b->ev_in);
     if (b->ev_out) cudaEventDestroy(b->ev_out);
     if (b->st) cudaStreamDestroy(b->st);
@@ -2099,6 +2103,20 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
         batch_release(b);
         delete b;
         return bfail(nullptr, e == cudaErrorMemoryAllocation ? VFD_ERR_OUT_OF_MEMORY : VFD_ERR_CUDA, msg);
+    }
+    {
+        std::vector<double *> mp;
+        std::vector<int> mc;
+        for (auto *w : b->worlds) {
+            mp.push_back(w->d_mass);
+            mc.push_back(MS_COUNT * w->nf);
+        }
+        if ((e = upload_vec(&b->d_mass_ptrs, mp)) != cudaSuccess || (e = upload_vec(&b->d_mass_counts, mc)) != cudaSuccess) {
+            std::string msg = std::string("batch setup: ") + cudaGetErrorString(e);
+            batch_release(b);
+            delete b;
+            return bfail(nullptr, VFD_ERR_CUDA, msg);
+        }
     }
     b->gens.assign(n_worlds, ~0ull);
     b->oj.swap(oj);
@@ -2233,8 +2251,7 @@ vfd_status vfd_batch_destroy(vfd_batch *b)
 static vfd_status batch_enqueue(vfd_batch *b, int n_substeps)
 {
     for (int s = 0; s < n_substeps; ++s) {
-        for (auto *w : b->worlds)
-            VFD_BCUDA(b, cudaMemsetAsync(w->d_mass, 0, sizeof(double) * MS_COUNT * w->nf, b->st));
+        VFD_BCUDA(b, launch_zero_blocks(b->d_mass_ptrs, b->d_mass_counts, (int)b->worlds.size(), b->st));
         for (int a = 0; a < 3; ++a) {
             if (b->use_rf[a])
                 VFD_BCUDA(b, launch_rf_groups(b->d_osjobs + a * b->njobs, b->rf[a], a, b->st));
