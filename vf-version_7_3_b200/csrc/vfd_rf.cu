@@ -580,8 +580,8 @@ constexpr int RF_WIN_FLOATS = 64 * 64;  // one warp's window buffer
 
 // W warps per CTA, each on its own tile (tiles of other jobs than the CTA's
 // first are empty, as in rf_col_kernel); no CTA barrier after set-up.
-template <int W, bool ZL>
-__global__ void __launch_bounds__(32 * W, 12 / W) rf_col_tma_kernel(const OsJob *__restrict__ jobs,
+template <int W, bool ZL, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB) rf_col_tma_kernel(const OsJob *__restrict__ jobs,
                                                                     const CUtensorMap *__restrict__ maps,
                                                                     const OsTileInfo *__restrict__ tiles)
 {
@@ -1180,7 +1180,7 @@ bool rf_encode_map(const OsJob &j, CUtensorMap *m)
     return tma_encode_3d(m, j.data, nx, ny, nz, sy, sz, 64, 1, 64);
 }
 
-template <int W, bool Z>
+template <int W, bool Z, int MINB>
 static cudaError_t launch_col_tma(const OsJob *jobs, const CUtensorMap *maps, const OsTileInfo *tiles, int nb,
                                   cudaStream_t st)
 {
@@ -1190,12 +1190,25 @@ static cudaError_t launch_col_tma(const OsJob *jobs, const CUtensorMap *maps, co
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev >= 0 && dev < 64 && !done[dev]) {
-        e = cudaFuncSetAttribute(rf_col_tma_kernel<W, Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        e = cudaFuncSetAttribute(rf_col_tma_kernel<W, Z, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)dyn);
         if (e != cudaSuccess) return e;
         done[dev] = 1;
     }
-    rf_col_tma_kernel<W, Z><<<nb, 32 * W, dyn, st>>>(jobs, maps, tiles);
+    rf_col_tma_kernel<W, Z, MINB><<<nb, 32 * W, dyn, st>>>(jobs, maps, tiles);
     return cudaSuccess;
+}
+
+// Resident 4-warp CTAs per SM the TMA y/z kernel is compiled for
+// (VFD_RF_YZ_MINB: 3 = 12 warps at 168 registers, 2 = 8 warps at 255).
+static int rf_yz_minb()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("VFD_RF_YZ_MINB");
+        v = (e && e[0] == '2') ? 2 : 3;
+    }
+    return v;
 }
 
 cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, int axis, cudaStream_t st,
@@ -1226,8 +1239,12 @@ cudaError_t launch_rf(const OsJob *jobs, const OsTileInfo *tiles, int ntiles, in
     } else if (axis == PASS_X) {
         rf_row_kernel<<<ntiles, 32, 0, st>>>(jobs, tiles);
     } else if (maps && W == 4) {
-        e = axis == PASS_Z ? launch_col_tma<4, true>(jobs, maps, tiles, nb, st)
-                           : launch_col_tma<4, false>(jobs, maps, tiles, nb, st);
+        if (rf_yz_minb() == 2)
+            e = axis == PASS_Z ? launch_col_tma<4, true, 2>(jobs, maps, tiles, nb, st)
+                               : launch_col_tma<4, false, 2>(jobs, maps, tiles, nb, st);
+        else
+            e = axis == PASS_Z ? launch_col_tma<4, true, 3>(jobs, maps, tiles, nb, st)
+                               : launch_col_tma<4, false, 3>(jobs, maps, tiles, nb, st);
         if (e != cudaSuccess) return e;
     } else {
         const bool z = axis == PASS_Z;
