@@ -416,6 +416,14 @@ vfd_status vfd_sample_field(vfd_world *w, int field, int stride, float scale, fl
  * output_utils.h:813-854), values with 9 significant digits. */
 vfd_status vfd_write_vtk(const float *field, int nx, int ny, int nz, const char *path);
 
+/* The reference's raw field writers (output_utils.h:21-128) for one host
+ * field: an 8-bit volume, v -> 255 if v >= 1, 0 if v <= 0, else floor(256 v)
+ * (writeNormalizedFloatRaw; append != 0 adds a frame to the file,
+ * writeNormalizedFloatRawFrames), and comma-separated values, one line per
+ * row and an empty line per z plane, 6 significant digits (writeFloatCsv). */
+vfd_status vfd_write_raw_normalized(const float *field, int nx, int ny, int nz, const char *path, int append);
+vfd_status vfd_write_csv(const float *field, int nx, int ny, int nz, const char *path);
+
 /* ---- diagnostics ------------------------------------------------------ */
 const char *vfd_status_string(vfd_status s);
 /* Last error message of this world (or of the last failed create when

@@ -1,5 +1,6 @@
 """The steps either side of the path: attractant gradients (F1), the compute
-part of sampleChem (F3), the legacy-VTK field writer (F4)."""
+part of sampleChem (F3), the field writers (F4: legacy VTK, the 8-bit
+normalised raw volume and the CSV dump of output_utils.h)."""
 import numpy as np
 import pytest
 
@@ -20,6 +21,34 @@ def test_vtk_writer_layout(tmp_path):
     rows = [list(map(float, ln.split())) for ln in lines[10:]]
     assert len(rows) == 6 and all(len(r) == 4 for r in rows)
     np.testing.assert_array_equal(np.array(rows, np.float32).reshape(2, 3, 4), f)
+
+
+def test_raw_normalized_writer(tmp_path):
+    """writeNormalizedFloatRaw (output_utils.h:86-103): 255 at or above 1, 0 at
+    or below 0, else floor(256 v); the frames variant appends."""
+    f = np.array([-1.0, 0.0, 0.001, 0.5, 0.999, 1.0, 2.0, 0.25, 0.75, 0.1, 0.3, 0.0039],
+                 np.float32).reshape(2, 2, 3)
+    p = tmp_path / "f.raw"
+    vfd.write_raw_normalized(f, p)
+    got = np.frombuffer(p.read_bytes(), np.uint8)
+    v = f.ravel()
+    ref = np.where(v >= 1.0, 255, np.where(v <= 0.0, 0, np.floor(v * np.float32(256.0)))).astype(np.uint8)
+    np.testing.assert_array_equal(got, ref)
+    vfd.write_raw_normalized(f, p, append=True)
+    assert p.read_bytes() == ref.tobytes() * 2
+
+
+def test_csv_writer_layout(tmp_path):
+    """writeFloatCsv (output_utils.h:41-66): one line per row, each value
+    followed by ", ", an empty line after each z plane."""
+    f = (np.arange(3 * 2 * 2, dtype=np.float32) * 0.125).reshape(2, 2, 3)
+    p = tmp_path / "f.csv"
+    vfd.write_csv(f, p)
+    lines = p.read_text().split("\n")
+    assert lines[0] == "0, 0.125, 0.25, " and lines[1] == "0.375, 0.5, 0.625, " and lines[2] == ""
+    assert lines[3] == "0.75, 0.875, 1, " and lines[5] == ""
+    vals = [float(x) for ln in lines if ln for x in ln.split(", ") if x]
+    np.testing.assert_array_equal(np.array(vals, np.float32), f.ravel())
 
 
 @pytest.mark.gpu

@@ -15,6 +15,7 @@
 //                    one line per row).
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <math.h>
 #include <stdio.h>
 
 #include "vfd.h"
@@ -93,4 +94,52 @@ extern "C" vfd_status vfd_write_vtk(const float *field, int nx, int ny, int nz, 
     const int bad = ferror(f);
     fclose(f);
     return bad ? VFD_ERR_INVALID_ARG : VFD_OK;
+}
+
+// The reference's raw field writers (output_utils.h:21-128), restated.
+// Normalised 8-bit volume: every voxel v -> 255 if v >= 1, 0 if v <= 0, else
+// floor(v * 256) (writeNormalizedFloatRaw; append = 1 adds a frame to an
+// existing file, writeNormalizedFloatRawFrames).
+extern "C" vfd_status vfd_write_raw_normalized(const float *field, int nx, int ny, int nz, const char *path,
+                                               int append)
+{
+    if (!field || !path || nx < 1 || ny < 1 || nz < 1) return VFD_ERR_INVALID_ARG;
+    FILE *f = fopen(path, append ? "ab" : "wb");
+    if (!f) return VFD_ERR_INVALID_ARG;
+    unsigned char buf[4096];
+    const size_t n = (size_t)nx * ny * nz;
+    size_t done = 0;
+    bool ok = true;
+    while (done < n && ok) {
+        const size_t m = n - done < sizeof(buf) ? n - done : sizeof(buf);
+        for (size_t i = 0; i < m; ++i) {
+            const float v = field[done + i];
+            buf[i] = v >= 1.0f ? 255 : (v <= 0.0f ? 0 : (unsigned char)floorf(v * 256.0f));
+        }
+        ok = fwrite(buf, 1, m, f) == m;
+        done += m;
+    }
+    ok = (fclose(f) == 0) && ok;
+    return ok ? VFD_OK : VFD_ERR_INVALID_ARG;
+}
+
+// Comma-separated values of a field (writeFloatCsv): one line per row (x
+// fastest, each value followed by ", "), an empty line after each z plane,
+// values with 6 significant digits (the iostream default).
+extern "C" vfd_status vfd_write_csv(const float *field, int nx, int ny, int nz, const char *path)
+{
+    if (!field || !path || nx < 1 || ny < 1 || nz < 1) return VFD_ERR_INVALID_ARG;
+    FILE *f = fopen(path, "w");
+    if (!f) return VFD_ERR_INVALID_ARG;
+    bool ok = true;
+    for (int z = 0; z < nz && ok; ++z) {
+        for (int y = 0; y < ny && ok; ++y) {
+            const float *r = field + (size_t)nx * (y + (size_t)ny * z);
+            for (int x = 0; x < nx; ++x) ok = ok && fprintf(f, "%g, ", (double)r[x]) > 0;
+            ok = ok && fputc('\n', f) != EOF;
+        }
+        ok = ok && fputc('\n', f) != EOF;
+    }
+    ok = (fclose(f) == 0) && ok;
+    return ok ? VFD_OK : VFD_ERR_INVALID_ARG;
 }

@@ -62,7 +62,7 @@ __device__ __forceinline__ void load_twiddles(float2 *tw, const float2 *src, int
 template <int NL, int TL, int MAXP, int MINB>
 __global__ void __launch_bounds__(NL *TL, MINB) r2c_x_kernel(const GenRowPass p)
 {
-    constexpr int NT = NL * TL, LS = NL + 1, NR = 2 * NL, NPG = NT / NR;
+    constexpr int NT = NL * TL, LS = NL + 1, NR = 2 * NL;
     extern __shared__ __align__(16) float2 gsm[];
     __shared__ double red[NT / 32];
     const int F = p.plan.F;
@@ -72,28 +72,32 @@ __global__ void __launch_bounds__(NL *TL, MINB) r2c_x_kernel(const GenRowPass p)
     load_twiddles<NL>(tw, p.tw, F, NT);
 
     const int r0 = blockIdx.x * NR;
-    const int rl = threadIdx.x % NR, pg = threadIdx.x / NR;
-    const int sidx = 2 * (rl % NL) + rl / NL;
-    const int row = r0 + rl;
-    const bool ok = row < p.nrows;
-    int r1 = 0, r2 = 0;
-    if (ok) {
-        r1 = row % p.rows_per_plane;
-        r2 = row / p.rows_per_plane;
-    }
-    bool rowin = ok;
-    if (ok && p.fuse_pad)
-        rowin = r1 >= p.box_lo[1] && r1 < p.box_hi[1] && r2 >= p.box_lo[2] && r2 < p.box_hi[2];
-    const float *src = p.rsrc + (int64_t)r1 * p.r_s1 + (int64_t)r2 * p.r_s2;
+    // real rows: warp w takes tile rows w, w + NT/32, ...; its lanes walk the
+    // row's positions, so every load instruction reads 128 contiguous bytes
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double acc = 0.0;
-    for (int x = pg; x < p.nload; x += NPG) {
-        float v = 0.0f;
-        if (rowin) {
-            v = __ldg(src + x);
-            if (p.fuse_pad) v = (x >= p.box_lo[0] && x < p.box_hi[0]) ? v - p.b : 0.0f;
+    for (int q = warp; q < NR; q += NT / 32) {
+        const int row = r0 + q;
+        const int sidx = 2 * (q % NL) + q / NL;
+        const bool ok = row < p.nrows;
+        int r1 = 0, r2 = 0;
+        if (ok) {
+            r1 = row % p.rows_per_plane;
+            r2 = row / p.rows_per_plane;
         }
-        Sf[x * 2 * LS + sidx] = v;
-        acc += (double)v;
+        bool rowin = ok;
+        if (ok && p.fuse_pad)
+            rowin = r1 >= p.box_lo[1] && r1 < p.box_hi[1] && r2 >= p.box_lo[2] && r2 < p.box_hi[2];
+        const float *src = p.rsrc + (int64_t)r1 * p.r_s1 + (int64_t)r2 * p.r_s2;
+        for (int x = lane; x < p.nload; x += 32) {
+            float v = 0.0f;
+            if (rowin) {
+                v = __ldg(src + x);
+                if (p.fuse_pad) v = (x >= p.box_lo[0] && x < p.box_hi[0]) ? v - p.b : 0.0f;
+            }
+            Sf[x * 2 * LS + sidx] = v;
+            acc += (double)v;
+        }
     }
     for (int i = p.nload * LS + threadIdx.x; i < F * LS; i += NT) S[i] = make_float2(0.f, 0.f);
     __syncthreads();
@@ -121,7 +125,7 @@ __global__ void __launch_bounds__(NL *TL, MINB) r2c_x_kernel(const GenRowPass p)
 template <int NL, int TL, int MAXP, int MINB>
 __global__ void __launch_bounds__(NL *TL, MINB) c2r_x_kernel(const GenRowPass p)
 {
-    constexpr int NT = NL * TL, LS = NL + 1, NR = 2 * NL, NPG = NT / NR;
+    constexpr int NT = NL * TL, LS = NL + 1, NR = 2 * NL;
     extern __shared__ __align__(16) float2 gsm[];
     __shared__ double red[NT / 32];
     const int F = p.plan.F;
@@ -152,20 +156,22 @@ __global__ void __launch_bounds__(NL *TL, MINB) c2r_x_kernel(const GenRowPass p)
     __syncthreads();
     fft_lines<MAXP, TL, NL, true>(S, p.plan, threadIdx.x % NL, threadIdx.x / NL, tw);
 
-    const int rl = threadIdx.x % NR, pg = threadIdx.x / NR;
-    const int sidx = 2 * (rl % NL) + rl / NL;
-    const int row = r0 + rl;
     double acc_leak = 0.0, acc_conv = 0.0, acc_out = 0.0;
     for (int i = threadIdx.x; i < (F - p.nstore) * NL; i += NT) {
         const float2 x = S[(p.nstore + i / NL) * LS + (i % NL)];
         acc_leak += (double)x.x + (double)x.y;
     }
-    if (row < p.nrows) {
+    // real rows: warp w stores tile rows w, w + NT/32, ...; lanes walk positions
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int q = warp; q < NR; q += NT / 32) {
+        const int row = r0 + q;
+        if (row >= p.nrows) continue;
+        const int sidx = 2 * (q % NL) + q / NL;
         const int r1 = row % p.rows_per_plane, r2 = row / p.rows_per_plane;
         float *dst = p.rdst + (int64_t)r1 * p.r_s1 + (int64_t)r2 * p.r_s2;
         // fused WHChemical::update: p = d + decay t, d = 0 (same row layout as the field)
         float *drow = (p.fuse_update && p.dchem) ? p.dchem + (int64_t)r1 * p.r_s1 + (int64_t)r2 * p.r_s2 : nullptr;
-        for (int x = pg; x < p.nstore; x += NPG) {
+        for (int x = lane; x < p.nstore; x += 32) {
             float t = Sf[x * 2 * LS + sidx];
             if (p.fuse_crop) {
                 acc_conv += (double)t;

@@ -46,7 +46,7 @@ EXPORTED = [
     "vfd_fft_diffuse3d_noalloc", "vfd_update_gradients", "vfd_sample_field", "vfd_write_vtk",
     "vfd_autotune", "vfd_world_tuning", "vfd_autotune_set", "vfd_autotune_clear",
     "vfd_set_spectrum", "vfd_set_boundary", "vfd_tick_update", "vfd_diffuse_update_host",
-    "vfd_batch_autotune", "vfd_window_spectrum",
+    "vfd_batch_autotune", "vfd_window_spectrum", "vfd_write_raw_normalized", "vfd_write_csv",
 ]
 
 PASS_METHODS = {0: "register_fft", 1: "overlap_save", 2: "full_line"}
@@ -154,6 +154,8 @@ def load(path=LIB_PATH):
     lib.vfd_update_gradients.argtypes = [P, P, P, P, P, P, P]
     lib.vfd_sample_field.argtypes = [P, C.c_int, C.c_int, C.c_float, P, P]
     lib.vfd_write_vtk.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_char_p]
+    lib.vfd_write_raw_normalized.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_int]
+    lib.vfd_write_csv.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_char_p]
     lib.vfd_stencil_window.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, P, C.c_int]
     lib.vfd_synth_field_device.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_float, C.c_float, P,
                                            C.c_size_t, P]
@@ -491,6 +493,21 @@ def window_spectrum(window, fft, centre=None, device=0):
     out = np.empty((fz, fy, fx // 2 + 1), np.complex64)
     _check(lib().vfd_window_spectrum(_ptr(w), kw, kh, kd, cx, cy, cz, fx, fy, fz, _ptr(out), device))
     return out
+
+
+def write_raw_normalized(field, path, append=False):
+    """8-bit normalised volume of a (nz, ny, nx) float32 field (the
+    reference's writeNormalizedFloatRaw / ...Frames)."""
+    a = np.ascontiguousarray(field, np.float32)
+    nz, ny, nx = a.shape
+    _check(lib().vfd_write_raw_normalized(_ptr(a), nx, ny, nz, str(path).encode(), int(bool(append))))
+
+
+def write_csv(field, path):
+    """Comma-separated values of a (nz, ny, nx) float32 field (writeFloatCsv)."""
+    a = np.ascontiguousarray(field, np.float32)
+    nz, ny, nx = a.shape
+    _check(lib().vfd_write_csv(_ptr(a), nx, ny, nz, str(path).encode()))
 
 
 def stencil_window(lam, gamma_dt, n_steps, R, device=0):
