@@ -29,6 +29,10 @@
 
 namespace vfd {
 
+// Global loads each thread keeps in flight before their shared-memory
+// stores in the load loops (the loops are otherwise bound by load latency).
+constexpr int kGU = 6;
+
 __device__ __forceinline__ double warp_sum_g(double v)
 {
 #pragma unroll
@@ -89,14 +93,24 @@ __global__ void __launch_bounds__(NL *TL, MINB) r2c_x_kernel(const GenRowPass p)
         if (ok && p.fuse_pad)
             rowin = r1 >= p.box_lo[1] && r1 < p.box_hi[1] && r2 >= p.box_lo[2] && r2 < p.box_hi[2];
         const float *src = p.rsrc + (int64_t)r1 * p.r_s1 + (int64_t)r2 * p.r_s2;
-        for (int x = lane; x < p.nload; x += 32) {
-            float v = 0.0f;
-            if (rowin) {
-                v = __ldg(src + x);
-                if (p.fuse_pad) v = (x >= p.box_lo[0] && x < p.box_hi[0]) ? v - p.b : 0.0f;
+        // kGU loads in flight per lane before their shared-memory stores
+        for (int x0 = lane; x0 < p.nload; x0 += 32 * kGU) {
+            float v[kGU];
+#pragma unroll
+            for (int u = 0; u < kGU; ++u) {
+                const int x = x0 + 32 * u;
+                v[u] = (rowin && x < p.nload) ? __ldg(src + x) : 0.0f;
             }
-            Sf[x * 2 * LS + sidx] = v;
-            acc += (double)v;
+#pragma unroll
+            for (int u = 0; u < kGU; ++u) {
+                const int x = x0 + 32 * u;
+                if (x < p.nload) {
+                    float w = v[u];
+                    if (p.fuse_pad) w = (rowin && x >= p.box_lo[0] && x < p.box_hi[0]) ? w - p.b : 0.0f;
+                    Sf[x * 2 * LS + sidx] = w;
+                    acc += (double)w;
+                }
+            }
         }
     }
     for (int i = p.nload * LS + threadIdx.x; i < F * LS; i += NT) S[i] = make_float2(0.f, 0.f);
@@ -136,22 +150,37 @@ __global__ void __launch_bounds__(NL *TL, MINB) c2r_x_kernel(const GenRowPass p)
     load_twiddles<NL>(tw, p.tw, F, NT);
 
     const int r0 = blockIdx.x * NR;
-    // rebuild z(k) = A(k) + i B(k) for every k from the Hermitian halves
-    for (int i = threadIdx.x; i < NL * Fh; i += NT) {
-        const int ln = i / Fh, k = i - ln * Fh;
-        const int ra = r0 + ln, rb = r0 + NL + ln;
-        float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
-        if (ra < p.nrows) {
-            const int s1 = ra % p.rows_per_plane, s2 = ra / p.rows_per_plane;
-            A = p.csrc[(int64_t)s1 * p.c_s1 + (int64_t)s2 * p.c_s2 + k];
+    // rebuild z(k) = A(k) + i B(k) for every k from the Hermitian halves:
+    // warp w takes line pairs w, w + NT/32, ...; its lanes walk k with kGU
+    // loads of each row in flight
+    {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for (int ln = warp; ln < NL; ln += NT / 32) {
+            const int ra = r0 + ln, rb = r0 + NL + ln;
+            const float2 *pa = nullptr, *pb = nullptr;
+            if (ra < p.nrows)
+                pa = p.csrc + (int64_t)(ra % p.rows_per_plane) * p.c_s1 + (int64_t)(ra / p.rows_per_plane) * p.c_s2;
+            if (rb < p.nrows)
+                pb = p.csrc + (int64_t)(rb % p.rows_per_plane) * p.c_s1 + (int64_t)(rb / p.rows_per_plane) * p.c_s2;
+            for (int k0 = lane; k0 < Fh; k0 += 32 * kGU) {
+                float2 A[kGU], B[kGU];
+#pragma unroll
+                for (int u = 0; u < kGU; ++u) {
+                    const int k = k0 + 32 * u;
+                    A[u] = (pa && k < Fh) ? pa[k] : make_float2(0.f, 0.f);
+                    B[u] = (pb && k < Fh) ? pb[k] : make_float2(0.f, 0.f);
+                }
+#pragma unroll
+                for (int u = 0; u < kGU; ++u) {
+                    const int k = k0 + 32 * u;
+                    if (k < Fh) {
+                        // z(k) = A + iB ; z(-k) = conj(A) + i conj(B)
+                        S[k * LS + ln] = make_float2(A[u].x - B[u].y, A[u].y + B[u].x);
+                        if (k > 0 && k < F - k) S[(F - k) * LS + ln] = make_float2(A[u].x + B[u].y, B[u].x - A[u].y);
+                    }
+                }
+            }
         }
-        if (rb < p.nrows) {
-            const int s1 = rb % p.rows_per_plane, s2 = rb / p.rows_per_plane;
-            B = p.csrc[(int64_t)s1 * p.c_s1 + (int64_t)s2 * p.c_s2 + k];
-        }
-        // z(k) = A + iB ; z(-k) = conj(A) + i conj(B)
-        S[k * LS + ln] = make_float2(A.x - B.y, A.y + B.x);
-        if (k > 0 && k < F - k) S[(F - k) * LS + ln] = make_float2(A.x + B.y, B.x - A.y);
     }
     __syncthreads();
     fft_lines<MAXP, TL, NL, true>(S, p.plan, threadIdx.x % NL, threadIdx.x / NL, tw);
@@ -212,8 +241,19 @@ __global__ void __launch_bounds__(NL *TL, MINB) c2c_kernel(const GenColPass p)
     const int ln = threadIdx.x % NL, pg = threadIdx.x / NL;
     const bool ok = (l0 + ln) < p.nlines;
     float2 *base = p.data + (int64_t)outer * p.outer_stride + l0 + ln;
-    for (int x = pg; x < p.nload; x += NPG)
-        S[x * LS + ln] = ok ? base[(int64_t)x * p.pos_stride] : make_float2(0.f, 0.f);
+    for (int x0 = pg; x0 < p.nload; x0 += NPG * kGU) {
+        float2 v[kGU];
+#pragma unroll
+        for (int u = 0; u < kGU; ++u) {
+            const int x = x0 + NPG * u;
+            v[u] = (ok && x < p.nload) ? base[(int64_t)x * p.pos_stride] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < kGU; ++u) {
+            const int x = x0 + NPG * u;
+            if (x < p.nload) S[x * LS + ln] = v[u];
+        }
+    }
     for (int i = p.nload * LS + threadIdx.x; i < F * LS; i += NT) S[i] = make_float2(0.f, 0.f);
     __syncthreads();
     const int line = threadIdx.x % NL, tj = threadIdx.x / NL;
