@@ -1167,8 +1167,12 @@ vfd_status vfd_set_boundary(vfd_world *w, int epi_boundary, const float *baselin
     return VFD_OK;
 }
 
-// Uploads the concatenated source list and deposit jobs when they changed.
-static vfd_status sync_sources(vfd_world *w)
+// Uploads the concatenated source list and deposit jobs when they changed,
+// ordered on stream `st` before the tick that follows.  The lists grow by
+// stream-ordered allocation (cudaMallocAsync / cudaFreeAsync), so a world
+// whose sources grow does not wait for work in flight on other streams (a
+// server reusing worlds keeps several rounds queued on the device).
+static vfd_status sync_sources(vfd_world *w, cudaStream_t st)
 {
     if (!w->src_dirty) return VFD_OK;
     int64_t total = 0;
@@ -1178,14 +1182,15 @@ static vfd_status sync_sources(vfd_world *w)
         total += w->src_count[f];
     }
     if (total > w->src_cap) {
-        cudaFree(w->d_src_idx);
-        cudaFree(w->d_src_amt);
+        if (w->d_src_idx) VFD_CUDA(w, cudaFreeAsync(w->d_src_idx, st));
+        if (w->d_src_amt) VFD_CUDA(w, cudaFreeAsync(w->d_src_amt, st));
         w->d_src_idx = nullptr;
         w->d_src_amt = nullptr;
         w->src_cap = 0;
-        VFD_CUDA(w, cudaMalloc(&w->d_src_idx, sizeof(int32_t) * total));
-        VFD_CUDA(w, cudaMalloc(&w->d_src_amt, sizeof(float) * total));
-        w->src_cap = total;
+        const int64_t cap = std::max<int64_t>(total, 2 * w->src_total);
+        VFD_CUDA(w, cudaMallocAsync(&w->d_src_idx, sizeof(int32_t) * cap, st));
+        VFD_CUDA(w, cudaMallocAsync(&w->d_src_amt, sizeof(float) * cap, st));
+        w->src_cap = cap;
     }
     std::vector<int32_t> hi(total);
     std::vector<float> ha(total);
@@ -1193,9 +1198,10 @@ static vfd_status sync_sources(vfd_world *w)
         std::copy(w->src_idx[f].begin(), w->src_idx[f].end(), hi.begin() + w->src_begin[f]);
         std::copy(w->src_amt[f].begin(), w->src_amt[f].end(), ha.begin() + w->src_begin[f]);
     }
+    // pageable sources: each copy returns once its data is staged
     if (total > 0) {
-        VFD_CUDA(w, cudaMemcpy(w->d_src_idx, hi.data(), sizeof(int32_t) * total, cudaMemcpyHostToDevice));
-        VFD_CUDA(w, cudaMemcpy(w->d_src_amt, ha.data(), sizeof(float) * total, cudaMemcpyHostToDevice));
+        VFD_CUDA(w, cudaMemcpyAsync(w->d_src_idx, hi.data(), sizeof(int32_t) * total, cudaMemcpyHostToDevice, st));
+        VFD_CUDA(w, cudaMemcpyAsync(w->d_src_amt, ha.data(), sizeof(float) * total, cudaMemcpyHostToDevice, st));
     }
     std::vector<DepositJob> jobs;
     for (int f = 0; f < w->nf; ++f) {
@@ -1219,7 +1225,7 @@ static vfd_status sync_sources(vfd_world *w)
         j.nvox = w->V;
         jobs.push_back(j);
     }
-    VFD_CUDA(w, cudaMemcpy(w->d_dep, jobs.data(), sizeof(DepositJob) * jobs.size(), cudaMemcpyHostToDevice));
+    VFD_CUDA(w, cudaMemcpyAsync(w->d_dep, jobs.data(), sizeof(DepositJob) * jobs.size(), cudaMemcpyHostToDevice, st));
     w->src_total = total;
     w->src_dirty = false;
     w->src_gen++;
@@ -1473,7 +1479,7 @@ vfd_status vfd_tick(vfd_world *w, int n_substeps, void *stream)
     if (!w) return VFD_ERR_INVALID_ARG;
     if (n_substeps < 1) return fail(w, VFD_ERR_INVALID_ARG, "n_substeps must be >= 1");
     DeviceGuard g(w->device);
-    vfd_status s = sync_sources(w);
+    vfd_status s = sync_sources(w, (cudaStream_t)stream);
     if (s != VFD_OK) return s;
     return enqueue_tick(w, -1, n_substeps, (cudaStream_t)stream);
 }
@@ -1486,7 +1492,7 @@ vfd_status vfd_tick_update(vfd_world *w, int n_substeps, float *const *dchem, co
     for (int f = 0; f < w->nf; ++f)
         if (!std::isfinite(decay[f])) return fail(w, VFD_ERR_INVALID_ARG, "decay must be finite");
     DeviceGuard g(w->device);
-    vfd_status s = sync_sources(w);
+    vfd_status s = sync_sources(w, (cudaStream_t)stream);
     if (s != VFD_OK) return s;
     const UpdateArgs upd{dchem, decay};
     return enqueue_tick(w, -1, n_substeps, (cudaStream_t)stream, &upd);
@@ -1847,7 +1853,7 @@ vfd_status vfd_diffuse_host(vfd_world *w, const float *const *host_in, float *co
     for (int f = 0; f < w->nf; ++f)
         if (!host_in[f] || !host_out[f]) return fail(w, VFD_ERR_INVALID_ARG, "NULL host buffer");
     DeviceGuard g(w->device);
-    vfd_status s = sync_sources(w);
+    vfd_status s = sync_sources(w, w->s_cmp);
     if (s != VFD_OK) return s;
     const size_t bytes = sizeof(float) * w->V;
     for (int f = 0; f < w->nf; ++f) {
@@ -1880,7 +1886,7 @@ vfd_status vfd_diffuse_update_host(vfd_world *w, float *const *host_p, float *co
         if (!std::isfinite(decay[f])) return fail(w, VFD_ERR_INVALID_ARG, "decay must be finite");
     }
     DeviceGuard g(w->device);
-    vfd_status s = sync_sources(w);
+    vfd_status s = sync_sources(w, w->s_cmp);
     if (s != VFD_OK) return s;
     const size_t bytes = sizeof(float) * w->V;
     if (host_d && !w->d_upd) VFD_CUDA(w, cudaMalloc(&w->d_upd, bytes * w->nf));
@@ -2281,7 +2287,7 @@ vfd_status vfd_batch_tick(vfd_batch *b, int n_substeps, void *stream)
     // launches its kernels directly and pays no capture.
     bool stale = b->graph_substeps != n_substeps;
     for (size_t i = 0; i < b->worlds.size(); ++i) {
-        vfd_status st = sync_sources(b->worlds[i]);
+        vfd_status st = sync_sources(b->worlds[i], b->st);
         if (st != VFD_OK) return bfail(b, st, b->worlds[i]->err);
         if (b->gens[i] != b->worlds[i]->src_gen) stale = true;
     }
