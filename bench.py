@@ -497,7 +497,8 @@ def run_cfg3(args, dev=0):
             "requests": {k: st[k] for k in ("submitted", "admitted", "completed", "rejected", "queued", "active",
                                             "rounds")},
             "device_busy_frac": st["device_s"] / elapsed if elapsed > 0 else None,
-            "hbm_peak_bytes": st["hbm_peak"], "busy_s": st["busy_s"], "device_s": st["device_s"]}
+            "hbm_peak_bytes": st["hbm_peak"], "busy_s": st["busy_s"], "device_s": st["device_s"],
+            "host_s": {"batch": st["host_batch_s"], "admit": st["host_admit_s"], "wait": st["host_wait_s"]}}
 
 
 def run_fft3d(c, dev, stream, steps=3):

@@ -350,6 +350,10 @@ typedef struct vfd_server_stats {
     double device_s;                    /* device time of the rounds (CUDA events) */
     double p50_completed_s, p99_completed_s;  /* over completed requests only */
     int64_t censored;
+    /* scheduler-thread time spent building batches, admitting requests
+     * (world creation or reuse, field and source set-up), and waiting for
+     * rounds to complete */
+    double host_batch_s, host_admit_s, host_wait_s;
 } vfd_server_stats;
 
 vfd_status vfd_server_create(int device, size_t hbm_budget_bytes, int max_active, int substeps_per_tick,

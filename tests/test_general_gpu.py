@@ -280,3 +280,34 @@ def test_stencil_window_at_reference_size(gpu, lam):
         assert er64 <= 1e-4 and er <= 1e-4
         # the two differ by what the reference's FP32 power adds
         assert abs(er - er64) <= 0.1 * er64 + REL_L2
+
+
+@pytest.mark.skipif(not oracle.ref_replay_available(), reason="oracle/_ref not built")
+def test_against_reference_kernels_on_the_human_scale_grid(gpu):
+    """The config-1 grid (512x256x384), one field with the widest config-1
+    kernel (sigma 1.95, radius 6), the reference's constant-VF padding: the
+    reference's own kernels + cuFFT on its power-of-two grid (1024x512x512,
+    snapTransformSize) against this library's separable path, and against
+    its general path on that same grid with the spectrum made by
+    vfd_window_spectrum (the drop-in's configuration)."""
+    nx, ny, nz = 512, 256, 384
+    sig, r = 1.95, 6
+    t = oracle.gauss_taps(sig, r)
+    win = np.einsum("z,y,x->zyx", t, t, t).astype(np.float32)
+    base, epi = 2e-4, 500
+    fft = (1024, 512, 512)
+    u = vfd.synth_field(0, 0, 6, (nz, ny, nx))
+    ref = oracle.ref_replay(u, fft, win, (r, r, r), epi, base)
+    ins = [(u, np.zeros(0, np.int32), np.zeros(0, np.float32))]
+    sep, _, _ = run(vfd.METHOD_SEPARABLE, (nx, ny, nz), [sig], [0.0], ins, pad_mode=1, epi=epi, base=[base])
+    e_sep = rel_l2(sep[0], ref)
+    spec = vfd.window_spectrum(win, fft)
+    params = [vfd.field_params(1.0, 0.0, radius=r, baseline=base)]
+    with vfd.World(nx, ny, nz, params, pad_mode=1, epi_boundary=epi, fft=fft, method=vfd.METHOD_FFT3D) as w:
+        w.set_spectrum(0, spec)
+        w.upload(0, u)
+        w.tick(1)
+        g3 = w.download(0)
+    e_g3 = rel_l2(g3, ref)
+    print(f"config-1 grid vs the reference's kernels + cuFFT: separable {e_sep:.3e}, general {e_g3:.3e}")
+    assert e_sep <= REL_L2 and e_g3 <= REL_L2

@@ -260,7 +260,12 @@ void complete_oldest(vfd_server *s)
     Round rd = std::move(s->inflight.front());
     s->inflight.pop_front();
     float ms = 0.0f;
+    const double tw = s->now();
     const bool ok = cudaEventSynchronize(rd.end) == cudaSuccess;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->st.host_wait_s += s->now() - tw;
+    }
     if (ok) cudaEventElapsedTime(&ms, rd.start, rd.end);
     s->ev_pool.push_back(rd.start);
     s->ev_pool.push_back(rd.end);
@@ -351,6 +356,17 @@ std::vector<std::shared_ptr<Request>> select_admissions(vfd_server *s, int occup
 std::vector<std::shared_ptr<Request>> admit_all(vfd_server *s, const std::vector<std::shared_ptr<Request>> &sel)
 {
     std::vector<std::shared_ptr<Request>> ok;
+    if (sel.empty()) return ok;
+    const double t0 = s->now();
+    struct Account {
+        vfd_server *s;
+        double t0;
+        ~Account()
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->st.host_admit_s += s->now() - t0;
+        }
+    } account{s, t0};
     for (auto &r : sel) {
         std::string msg;
         bool reused = false;
@@ -412,7 +428,13 @@ void scheduler(vfd_server *s)
             s->batch = nullptr;
             std::vector<vfd_world *> ws;
             for (auto &r : s->active) ws.push_back(r->world);
-            if (vfd_batch_create(ws.data(), (int)ws.size(), &s->batch) != VFD_OK) {
+            const double tb = s->now();
+            const vfd_status bs = vfd_batch_create(ws.data(), (int)ws.size(), &s->batch);
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->st.host_batch_s += s->now() - tb;
+            }
+            if (bs != VFD_OK) {
                 const std::string msg = vfd_batch_last_error(nullptr);
                 complete_all(s);
                 for (auto &r : s->active) {

@@ -103,7 +103,8 @@ class ServerStats(C.Structure):
                 ("p50_latency_s", C.c_double), ("p99_latency_s", C.c_double),
                 ("mean_latency_s", C.c_double), ("hbm_in_use", C.c_size_t), ("hbm_peak", C.c_size_t),
                 ("device_s", C.c_double), ("p50_completed_s", C.c_double), ("p99_completed_s", C.c_double),
-                ("censored", C.c_int64)]
+                ("censored", C.c_int64), ("host_batch_s", C.c_double), ("host_admit_s", C.c_double),
+                ("host_wait_s", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
