@@ -221,13 +221,14 @@ static bool rf_enabled()
 // indices in the tiles are positions in `jobs`.
 static cudaError_t build_rf_groups(const OsJob *jobs, int n, std::vector<RfGroup> &out)
 {
-    std::vector<OsTileInfo> t;
-    for (int i = 0; i < n; ++i) rf_append_tiles(jobs[i], i, t);
-    if (t.empty()) return cudaSuccess;
     // CTAs start in tile order: grouping tiles by radius keeps the warps
-    // resident together on one compiled variant (instruction-cache locality)
-    std::stable_sort(t.begin(), t.end(),
-                     [&](const OsTileInfo &a, const OsTileInfo &b) { return jobs[a.job].r < jobs[b.job].r; });
+    // resident together on one compiled variant (instruction-cache locality);
+    // jobs are bucketed by radius (1..RF_RMAX), job order kept within a radius
+    std::vector<OsTileInfo> t;
+    for (int r = 1; r <= RF_RMAX; ++r)
+        for (int i = 0; i < n; ++i)
+            if (jobs[i].r == r || (r == RF_RMAX && (jobs[i].r < 1 || jobs[i].r > RF_RMAX))) rf_append_tiles(jobs[i], i, t);
+    if (t.empty()) return cudaSuccess;
     // CTAs of W warps: each job's run of tiles padded to a multiple of W
     const int W = rf_cta_warps(jobs[0].kind);
     if (W > 1) {
@@ -354,6 +355,7 @@ struct vfd_world {
     float *d_P = nullptr;            // full real grid scratch (plain)
     std::vector<float> k0;           // K(0,0,0) = sum of the window, per field
     float *d_upd = nullptr;          // vfd_diffuse_update_host: the fields' dChem on the device
+    std::vector<OsJob> oj_host;      // [axis][nf] overlap-save jobs (host copy, reused by batches)
 
     std::string err;
 };
@@ -828,6 +830,7 @@ static vfd_status world_create(const vfd_world_desc *d, int device, const ShapeC
                 tb += w->os_tiles[a][f];
             }
         }
+        w->oj_host.assign(oj.begin(), oj.end());
         for (int a = 0; a < 3; ++a)
             for (int f = 0; f < w->nf; ++f) oj.push_back(make_os_job(w, f, a, 0));
         if ((e = os_prepare()) != cudaSuccess) return bail(e, "overlap-save twiddles");
@@ -1998,20 +2001,41 @@ static void batch_release(vfd_batch *b)
 
 extern "C" {
 
+// Whether every job of axis a (oj: [axis][njobs]) can take the register-FFT
+// pass and every world allows it there.
+static bool batch_rf_possible(const vfd_batch *b, const std::vector<OsJob> &oj, int a)
+{
+    if (!rf_enabled() || !b->use_os[a]) return false;
+    for (auto *w : b->worlds)
+        if (!w->allow_rf[a]) return false;
+    for (int i = 0; i < b->njobs; ++i)
+        if (!rf_eligible(oj[(size_t)a * b->njobs + i])) return false;
+    return true;
+}
+
 // Register-FFT groups of every axis whose jobs (oj: [axis][njobs]) are all eligible.
 static cudaError_t batch_rf_setup(vfd_batch *b, const std::vector<OsJob> &oj)
 {
     if (!rf_enabled()) return cudaSuccess;
     for (int a = 0; a < 3; ++a) {
-        if (!b->use_os[a]) continue;
-        bool ok = true;
-        for (auto *w : b->worlds) ok = ok && w->allow_rf[a];
-        for (int i = 0; i < b->njobs; ++i) ok = ok && rf_eligible(oj[(size_t)a * b->njobs + i]);
-        if (!ok) continue;
+        if (!batch_rf_possible(b, oj, a)) continue;
         cudaError_t e = rf_prepare();
         if (e == cudaSuccess) e = build_rf_groups(&oj[(size_t)a * b->njobs], b->njobs, b->rf[a]);
         if (e != cudaSuccess) return e;
         b->use_rf[a] = true;
+    }
+    return cudaSuccess;
+}
+
+// Overlap-save tile lists for the axes that run that pass but have none yet.
+static cudaError_t batch_os_fill(vfd_batch *b, const std::vector<OsJob> &oj)
+{
+    for (int a = 0; a < 3; ++a) {
+        if (b->use_rf[a] || !b->use_os[a] || b->d_os_tiles[a]) continue;
+        std::vector<OsTileInfo> ti;
+        for (int i = 0; i < b->njobs; ++i) os_append_tiles(oj[(size_t)a * b->njobs + i], i, ti);
+        cudaError_t e = upload_vec(&b->d_os_tiles[a], ti);
+        if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
@@ -2076,11 +2100,22 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
             int tb = 0;
             for (auto *w : b->worlds)
                 for (int f = 0; f < w->nf; ++f) {
-                    oj.push_back(make_os_job(w, f, a, tb));
-                    os_append_tiles(oj.back(), (int)(oj.size() - 1 - (size_t)a * b->njobs), tile_info[a]);
+                    if (w->oj_host.size() == (size_t)3 * w->nf) {
+                        oj.push_back(w->oj_host[(size_t)a * w->nf + f]);  // the world's own job, re-based
+                        oj.back().tile_begin = tb;
+                    } else {
+                        oj.push_back(make_os_job(w, f, a, tb));
+                    }
                     tb += os_field_tiles(oj.back());
                 }
             b->os_tiles[a] = tb;
+        }
+        // the overlap-save tile lists only for axes the register-FFT pass
+        // cannot take (a server rebuilds its batch whenever the active set
+        // changes; autotuning builds the others when it times that pass)
+        for (int a = 0; a < 3; ++a) {
+            if (batch_rf_possible(b, oj, a)) continue;
+            for (int i = 0; i < b->njobs; ++i) os_append_tiles(oj[(size_t)a * b->njobs + i], i, tile_info[a]);
         }
     }
     DeviceGuard g(b->device);
@@ -2089,10 +2124,10 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
         if ((e2 = os_prepare()) != cudaSuccess ||
             (e2 = cudaMalloc(&b->d_osjobs, sizeof(OsJob) * oj.size())) != cudaSuccess ||
             (e2 = cudaMemcpy(b->d_osjobs, oj.data(), sizeof(OsJob) * oj.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
-            (e2 = upload_vec(&b->d_os_tiles[0], tile_info[0])) != cudaSuccess ||
-            (e2 = upload_vec(&b->d_os_tiles[1], tile_info[1])) != cudaSuccess ||
-            (e2 = upload_vec(&b->d_os_tiles[2], tile_info[2])) != cudaSuccess ||
-            (e2 = batch_rf_setup(b, oj)) != cudaSuccess) {
+            (!tile_info[0].empty() && (e2 = upload_vec(&b->d_os_tiles[0], tile_info[0])) != cudaSuccess) ||
+            (!tile_info[1].empty() && (e2 = upload_vec(&b->d_os_tiles[1], tile_info[1])) != cudaSuccess) ||
+            (!tile_info[2].empty() && (e2 = upload_vec(&b->d_os_tiles[2], tile_info[2])) != cudaSuccess) ||
+            (e2 = batch_rf_setup(b, oj)) != cudaSuccess || (e2 = batch_os_fill(b, oj)) != cudaSuccess) {
             std::string msg = std::string("batch os jobs: ") + cudaGetErrorString(e2);
             batch_release(b);
             delete b;
@@ -2197,9 +2232,14 @@ vfd_status vfd_batch_autotune(vfd_batch *b, int reps, vfd_axis_tuning *out3)
         struct Cand {
             int method, minb;
         };
+        if (b->can_os[a] && !b->d_os_tiles[a] && !b->oj.empty()) {
+            std::vector<OsTileInfo> ti;
+            for (int i = 0; i < b->njobs; ++i) os_append_tiles(b->oj[(size_t)a * b->njobs + i], i, ti);
+            if (upload_vec(&b->d_os_tiles[a], ti) != cudaSuccess) b->d_os_tiles[a] = nullptr;
+        }
         std::vector<Cand> cands;
         if (rf_ok) cands.push_back({PASS_METHOD_RF, 0});
-        if (b->can_os[a]) {
+        if (b->can_os[a] && b->d_os_tiles[a]) {
             cands.push_back({PASS_METHOD_OS, 3});
             cands.push_back({PASS_METHOD_OS, 4});
         }
