@@ -205,6 +205,27 @@ struct RfGroup {
     int ntiles = 0;
     OsTileInfo *d_tiles = nullptr;
     CUtensorMap *d_maps = nullptr;  // y / z: one TMA map per job (NULL: direct loads)
+    bool owned = true;              // false: the arrays live in their owner's arena
+};
+
+// A register-FFT launch's arrays on the host, before they are placed.
+struct RfGroupHost {
+    std::vector<OsTileInfo> tiles;
+    std::vector<CUtensorMap> maps;
+};
+
+// Device arrays of one object in a single allocation: staged on the host,
+// then one cudaMalloc and one copy (a server builds a batch every time its
+// active set changes; one allocation and copy instead of a dozen).
+struct ArenaBuilder {
+    std::vector<unsigned char> host;
+    size_t add(const void *p, size_t bytes, size_t align = 256)
+    {
+        const size_t off = (host.size() + align - 1) & ~(align - 1);
+        host.resize(off + bytes);
+        if (bytes) memcpy(host.data() + off, p, bytes);
+        return off;
+    }
 };
 
 static bool rf_enabled()
@@ -217,9 +238,9 @@ static bool rf_enabled()
     return on == 1;
 }
 
-// Tiles of jobs[0..n) (all rf-eligible) for one launch, uploaded.  Job
-// indices in the tiles are positions in `jobs`.
-static cudaError_t build_rf_groups(const OsJob *jobs, int n, std::vector<RfGroup> &out)
+// Tiles (and TMA maps) of jobs[0..n) (all rf-eligible) for one launch, on
+// the host.  Job indices in the tiles are positions in `jobs`.
+static void rf_group_host(const OsJob *jobs, int n, RfGroupHost &h)
 {
     // CTAs start in tile order: grouping tiles by radius keeps the warps
     // resident together on one compiled variant (instruction-cache locality);
@@ -228,7 +249,7 @@ static cudaError_t build_rf_groups(const OsJob *jobs, int n, std::vector<RfGroup
     for (int r = 1; r <= RF_RMAX; ++r)
         for (int i = 0; i < n; ++i)
             if (jobs[i].r == r || (r == RF_RMAX && (jobs[i].r < 1 || jobs[i].r > RF_RMAX))) rf_append_tiles(jobs[i], i, t);
-    if (t.empty()) return cudaSuccess;
+    if (t.empty()) return;
     // CTAs of W warps: each job's run of tiles padded to a multiple of W
     const int W = rf_cta_warps(jobs[0].kind);
     if (W > 1) {
@@ -241,9 +262,6 @@ static cudaError_t build_rf_groups(const OsJob *jobs, int n, std::vector<RfGroup
         }
         t.swap(p);
     }
-    RfGroup g;
-    g.r = 0;
-    g.ntiles = (int)t.size();
     // TMA tensor maps (x: two per job, y / z: one) when every job's layout
     // allows them; the CTA widths the TMA kernels take (x 2 warps, y / z 4)
     std::vector<CUtensorMap> maps;
@@ -254,6 +272,21 @@ static cudaError_t build_rf_groups(const OsJob *jobs, int n, std::vector<RfGroup
         for (int i = 0; i < n && !maps.empty(); ++i)
             if (!rf_encode_map(jobs[i], &maps[(size_t)i * per])) maps.clear();
     }
+    h.tiles.swap(t);
+    h.maps.swap(maps);
+}
+
+// rf_group_host, uploaded to arrays of its own.
+static cudaError_t build_rf_groups(const OsJob *jobs, int n, std::vector<RfGroup> &out)
+{
+    RfGroupHost h;
+    rf_group_host(jobs, n, h);
+    if (h.tiles.empty()) return cudaSuccess;
+    const std::vector<OsTileInfo> &t = h.tiles;
+    const std::vector<CUtensorMap> &maps = h.maps;
+    RfGroup g;
+    g.r = 0;
+    g.ntiles = (int)t.size();
     cudaError_t e = cudaMalloc(&g.d_tiles, sizeof(OsTileInfo) * t.size());
     if (e == cudaSuccess) e = cudaMemcpy(g.d_tiles, t.data(), sizeof(OsTileInfo) * t.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !maps.empty()) {
@@ -272,10 +305,11 @@ static cudaError_t build_rf_groups(const OsJob *jobs, int n, std::vector<RfGroup
 
 static void free_rf_groups(std::vector<RfGroup> &g)
 {
-    for (auto &x : g) {
-        cudaFree(x.d_tiles);
-        cudaFree(x.d_maps);
-    }
+    for (auto &x : g)
+        if (x.owned) {
+            cudaFree(x.d_tiles);
+            cudaFree(x.d_maps);
+        }
     g.clear();
 }
 
@@ -1956,6 +1990,8 @@ struct vfd_batch {
     std::vector<uint64_t> gens;
     double **d_mass_ptrs = nullptr;  // every world's accounting block, zeroed per substep in one launch
     int *d_mass_counts = nullptr;
+    unsigned char *d_arena = nullptr;  // the arrays set up at creation, in one allocation
+    bool os_tiles_owned[3] = {true, true, true};
     std::vector<OsJob> oj;       // host copy of the overlap-save jobs ([axis][njobs])
     bool can_os[3] = {false, false, false};
     float tuned_ms[3] = {0.0f, 0.0f, 0.0f};
@@ -1985,14 +2021,11 @@ static void batch_release(vfd_batch *b)
     cudaSetDevice(b->device);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
-    cudaFree(b->d_jobs);
-    cudaFree(b->d_osjobs);
     for (int a = 0; a < 3; ++a) {
-        cudaFree(b->d_os_tiles[a]);
+        if (b->os_tiles_owned[a]) cudaFree(b->d_os_tiles[a]);
         free_rf_groups(b->rf[a]);
     }
-    cudaFree(b->d_mass_ptrs);
-    cudaFree(b->d_mass_counts);
+    cudaFree(b->d_arena);  // d_jobs, d_osjobs, the mass arrays and the arena-placed tiles
     if (b->ev_in) cudaEventDestroy(b->ev_in);
     if (b->ev_out) cudaEventDestroy(b->ev_out);
     if (b->st) cudaStreamDestroy(b->st);
@@ -2013,32 +2046,7 @@ static bool batch_rf_possible(const vfd_batch *b, const std::vector<OsJob> &oj, 
     return true;
 }
 
-// Register-FFT groups of every axis whose jobs (oj: [axis][njobs]) are all eligible.
-static cudaError_t batch_rf_setup(vfd_batch *b, const std::vector<OsJob> &oj)
-{
-    if (!rf_enabled()) return cudaSuccess;
-    for (int a = 0; a < 3; ++a) {
-        if (!batch_rf_possible(b, oj, a)) continue;
-        cudaError_t e = rf_prepare();
-        if (e == cudaSuccess) e = build_rf_groups(&oj[(size_t)a * b->njobs], b->njobs, b->rf[a]);
-        if (e != cudaSuccess) return e;
-        b->use_rf[a] = true;
-    }
-    return cudaSuccess;
-}
 
-// Overlap-save tile lists for the axes that run that pass but have none yet.
-static cudaError_t batch_os_fill(vfd_batch *b, const std::vector<OsJob> &oj)
-{
-    for (int a = 0; a < 3; ++a) {
-        if (b->use_rf[a] || !b->use_os[a] || b->d_os_tiles[a]) continue;
-        std::vector<OsTileInfo> ti;
-        for (int i = 0; i < b->njobs; ++i) os_append_tiles(oj[(size_t)a * b->njobs + i], i, ti);
-        cudaError_t e = upload_vec(&b->d_os_tiles[a], ti);
-        if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
-}
 
 vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **out)
 {
@@ -2110,33 +2118,43 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
                 }
             b->os_tiles[a] = tb;
         }
-        // the overlap-save tile lists only for axes the register-FFT pass
-        // cannot take (a server rebuilds its batch whenever the active set
-        // changes; autotuning builds the others when it times that pass)
-        for (int a = 0; a < 3; ++a) {
-            if (batch_rf_possible(b, oj, a)) continue;
+    }
+    // Per axis: the register-FFT pass when every job and world allows it,
+    // else the overlap-save pass (its tile list built only then: a server
+    // rebuilds its batch whenever the active set changes; autotuning builds
+    // the others when it times that pass), else the full-line pass.
+    RfGroupHost rfh[3];
+    for (int a = 0; a < 3 && !oj.empty(); ++a) {
+        if (batch_rf_possible(b, oj, a)) {
+            rf_group_host(&oj[(size_t)a * b->njobs], b->njobs, rfh[a]);
+            if (!rfh[a].tiles.empty()) continue;
+        }
+        if (b->use_os[a])
             for (int i = 0; i < b->njobs; ++i) os_append_tiles(oj[(size_t)a * b->njobs + i], i, tile_info[a]);
-        }
     }
+    std::vector<double *> mp;
+    std::vector<int> mc;
+    for (auto *w : b->worlds) {
+        mp.push_back(w->d_mass);
+        mc.push_back(MS_COUNT * w->nf);
+    }
+    ArenaBuilder ar;
+    const size_t o_jobs = ar.add(jobs.data(), sizeof(AxisJob) * jobs.size());
+    const size_t o_oj = ar.add(oj.data(), sizeof(OsJob) * oj.size());
+    size_t o_ost[3], o_rft[3], o_rfm[3];
+    for (int a = 0; a < 3; ++a) {
+        o_ost[a] = ar.add(tile_info[a].data(), sizeof(OsTileInfo) * tile_info[a].size());
+        o_rft[a] = ar.add(rfh[a].tiles.data(), sizeof(OsTileInfo) * rfh[a].tiles.size());
+        o_rfm[a] = ar.add(rfh[a].maps.data(), sizeof(CUtensorMap) * rfh[a].maps.size());
+    }
+    const size_t o_mp = ar.add(mp.data(), sizeof(double *) * mp.size());
+    const size_t o_mc = ar.add(mc.data(), sizeof(int) * mc.size());
     DeviceGuard g(b->device);
-    if (!oj.empty()) {
-        cudaError_t e2 = cudaSuccess;
-        if ((e2 = os_prepare()) != cudaSuccess ||
-            (e2 = cudaMalloc(&b->d_osjobs, sizeof(OsJob) * oj.size())) != cudaSuccess ||
-            (e2 = cudaMemcpy(b->d_osjobs, oj.data(), sizeof(OsJob) * oj.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
-            (!tile_info[0].empty() && (e2 = upload_vec(&b->d_os_tiles[0], tile_info[0])) != cudaSuccess) ||
-            (!tile_info[1].empty() && (e2 = upload_vec(&b->d_os_tiles[1], tile_info[1])) != cudaSuccess) ||
-            (!tile_info[2].empty() && (e2 = upload_vec(&b->d_os_tiles[2], tile_info[2])) != cudaSuccess) ||
-            (e2 = batch_rf_setup(b, oj)) != cudaSuccess || (e2 = batch_os_fill(b, oj)) != cudaSuccess) {
-            std::string msg = std::string("batch os jobs: ") + cudaGetErrorString(e2);
-            batch_release(b);
-            delete b;
-            return bfail(nullptr, VFD_ERR_CUDA, msg);
-        }
-    }
-    cudaError_t e;
-    if ((e = cudaMalloc(&b->d_jobs, sizeof(AxisJob) * jobs.size())) != cudaSuccess ||
-        (e = cudaMemcpy(b->d_jobs, jobs.data(), sizeof(AxisJob) * jobs.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
+    cudaError_t e = cudaSuccess;
+    if ((!oj.empty() && (e = os_prepare()) != cudaSuccess) ||
+        ((rfh[0].tiles.size() + rfh[1].tiles.size() + rfh[2].tiles.size()) > 0 && (e = rf_prepare()) != cudaSuccess) ||
+        (e = cudaMalloc(&b->d_arena, ar.host.size())) != cudaSuccess ||
+        (e = cudaMemcpy(b->d_arena, ar.host.data(), ar.host.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming)) != cudaSuccess) {
@@ -2145,20 +2163,26 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
         delete b;
         return bfail(nullptr, e == cudaErrorMemoryAllocation ? VFD_ERR_OUT_OF_MEMORY : VFD_ERR_CUDA, msg);
     }
-    {
-        std::vector<double *> mp;
-        std::vector<int> mc;
-        for (auto *w : b->worlds) {
-            mp.push_back(w->d_mass);
-            mc.push_back(MS_COUNT * w->nf);
+    unsigned char *base = b->d_arena;
+    b->d_jobs = reinterpret_cast<AxisJob *>(base + o_jobs);
+    b->d_osjobs = oj.empty() ? nullptr : reinterpret_cast<OsJob *>(base + o_oj);
+    for (int a = 0; a < 3; ++a) {
+        if (!tile_info[a].empty()) {
+            b->d_os_tiles[a] = reinterpret_cast<OsTileInfo *>(base + o_ost[a]);
+            b->os_tiles_owned[a] = false;
         }
-        if ((e = upload_vec(&b->d_mass_ptrs, mp)) != cudaSuccess || (e = upload_vec(&b->d_mass_counts, mc)) != cudaSuccess) {
-            std::string msg = std::string("batch setup: ") + cudaGetErrorString(e);
-            batch_release(b);
-            delete b;
-            return bfail(nullptr, VFD_ERR_CUDA, msg);
+        if (!rfh[a].tiles.empty()) {
+            RfGroup rg;
+            rg.ntiles = (int)rfh[a].tiles.size();
+            rg.d_tiles = reinterpret_cast<OsTileInfo *>(base + o_rft[a]);
+            rg.d_maps = rfh[a].maps.empty() ? nullptr : reinterpret_cast<CUtensorMap *>(base + o_rfm[a]);
+            rg.owned = false;
+            b->rf[a].push_back(rg);
+            b->use_rf[a] = true;
         }
     }
+    b->d_mass_ptrs = reinterpret_cast<double **>(base + o_mp);
+    b->d_mass_counts = reinterpret_cast<int *>(base + o_mc);
     b->gens.assign(n_worlds, ~0ull);
     b->oj.swap(oj);
     *out = b;
@@ -2236,6 +2260,7 @@ vfd_status vfd_batch_autotune(vfd_batch *b, int reps, vfd_axis_tuning *out3)
             std::vector<OsTileInfo> ti;
             for (int i = 0; i < b->njobs; ++i) os_append_tiles(b->oj[(size_t)a * b->njobs + i], i, ti);
             if (upload_vec(&b->d_os_tiles[a], ti) != cudaSuccess) b->d_os_tiles[a] = nullptr;
+            b->os_tiles_owned[a] = true;
         }
         std::vector<Cand> cands;
         if (rf_ok) cands.push_back({PASS_METHOD_RF, 0});
