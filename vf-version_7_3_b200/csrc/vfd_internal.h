@@ -65,4 +65,9 @@ cudaError_t launch_sample(const float *src, int nx, int ny, int nz, int stride, 
 
 void note_launch();
 
+// Unique id of the calling thread's current CUDA context (0 when the driver
+// does not tell): caches of device pointers are keyed by it, because a
+// device reset loads the library into a new context.
+unsigned long long current_context_id();
+
 }  // namespace vfd

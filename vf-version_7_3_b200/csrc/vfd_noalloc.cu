@@ -52,7 +52,7 @@ struct NoAllocSlot {
 static NoAllocSlot g_noalloc[kMaxDevices];
 
 // Unique id of the calling thread's current context (0 when unavailable).
-static unsigned long long current_context_id()
+unsigned long long current_context_id()
 {
     static PFN_cuCtxGetCurrent_v4000 get_cur = nullptr;
     static PFN_cuCtxGetId_v12000 get_id = nullptr;

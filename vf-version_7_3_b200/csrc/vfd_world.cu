@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -2014,6 +2015,73 @@ static vfd_status bfail(vfd_batch *b, vfd_status s, const std::string &msg)
                          std::string(#call) + ": " + cudaGetErrorString(e_));               \
     } while (0)
 
+// Arenas and streams of destroyed batches, kept per device for the next
+// batch (a server creates a batch at every change of its active set):
+// destroying a batch frees nothing on the device, creating one allocates
+// only when no kept arena is large enough.
+struct BatchCache {
+    std::mutex mu;
+    unsigned long long ctx[64] = {};                    // context the kept items belong to
+    std::multimap<size_t, unsigned char *> arenas[64];  // by capacity
+    std::vector<std::array<void *, 3>> streams[64];     // stream, ev_in, ev_out
+};
+static BatchCache g_bcache;
+// capacity and context of every arena handed out (under g_bcache.mu)
+static std::map<unsigned char *, std::pair<size_t, unsigned long long>> g_arena_cap;
+
+// Forgets what was kept for `dev` if it belongs to another context than the
+// current one (after a device reset; the memory went with that context).
+static void bcache_check_context(int dev)
+{
+    const unsigned long long c = current_context_id();
+    if (c == 0 || g_bcache.ctx[dev] == c) return;
+    for (auto &kv : g_bcache.arenas[dev]) g_arena_cap.erase(kv.second);
+    g_bcache.arenas[dev].clear();
+    g_bcache.streams[dev].clear();
+    g_bcache.ctx[dev] = c;
+}
+
+static cudaError_t take_arena(int dev, size_t bytes, unsigned char **out)
+{
+    {
+        std::lock_guard<std::mutex> lk(g_bcache.mu);
+        if (dev >= 0 && dev < 64) {
+            bcache_check_context(dev);
+            auto &m = g_bcache.arenas[dev];
+            auto it = m.lower_bound(bytes);
+            if (it != m.end() && it->first <= 4 * bytes + (1 << 20)) {
+                *out = it->second;
+                m.erase(it);
+                return cudaSuccess;
+            }
+        }
+    }
+    const size_t cap = bytes + bytes / 4 + 4096;
+    cudaError_t e = cudaMalloc(out, cap);
+    if (e == cudaSuccess) {
+        const unsigned long long c = current_context_id();
+        std::lock_guard<std::mutex> lk(g_bcache.mu);
+        g_arena_cap[*out] = {cap, c};
+    }
+    return e;
+}
+
+static void give_arena(int dev, unsigned char *p)
+{
+    if (!p) return;
+    const unsigned long long c = current_context_id();
+    std::lock_guard<std::mutex> lk(g_bcache.mu);
+    auto it = g_arena_cap.find(p);
+    const bool keep = dev >= 0 && dev < 64 && it != g_arena_cap.end() && it->second.second == c && c != 0 &&
+                      g_bcache.ctx[dev] == c && g_bcache.arenas[dev].size() < 64;
+    if (!keep) {
+        if (it != g_arena_cap.end()) g_arena_cap.erase(it);
+        cudaFree(p);
+        return;
+    }
+    g_bcache.arenas[dev].insert({it->second.first, p});
+}
+
 static void batch_release(vfd_batch *b)
 {
     int prev = 0;
@@ -2025,10 +2093,25 @@ static void batch_release(vfd_batch *b)
         if (b->os_tiles_owned[a]) cudaFree(b->d_os_tiles[a]);
         free_rf_groups(b->rf[a]);
     }
-    cudaFree(b->d_arena);  // d_jobs, d_osjobs, the mass arrays and the arena-placed tiles
-    if (b->ev_in) cudaEventDestroy(b->ev_in);
-    if (b->ev_out) cudaEventDestroy(b->ev_out);
-    if (b->st) cudaStreamDestroy(b->st);
+    // d_jobs, d_osjobs, the mass arrays and the arena-placed tiles: the
+    // arena is kept for the next batch on this device (the batch's work is
+    // complete when it is destroyed)
+    if (b->d_arena) cudaStreamSynchronize(b->st);
+    give_arena(b->device, b->d_arena);
+    bool kept = false;
+    if (b->st && b->ev_in && b->ev_out && b->device >= 0 && b->device < 64) {
+        const unsigned long long c = current_context_id();
+        std::lock_guard<std::mutex> lk(g_bcache.mu);
+        if (c != 0 && g_bcache.ctx[b->device] == c && g_bcache.streams[b->device].size() < 64) {
+            g_bcache.streams[b->device].push_back({(void *)b->st, (void *)b->ev_in, (void *)b->ev_out});
+            kept = true;
+        }
+    }
+    if (!kept) {
+        if (b->ev_in) cudaEventDestroy(b->ev_in);
+        if (b->ev_out) cudaEventDestroy(b->ev_out);
+        if (b->st) cudaStreamDestroy(b->st);
+    }
     cudaSetDevice(prev);
 }
 
@@ -2047,6 +2130,29 @@ static bool batch_rf_possible(const vfd_batch *b, const std::vector<OsJob> &oj, 
 }
 
 
+
+// The batch's stream and events: kept ones of this device, or new.
+static cudaError_t take_stream(vfd_batch *b)
+{
+    if (b->device >= 0 && b->device < 64) {
+        std::lock_guard<std::mutex> lk(g_bcache.mu);
+        bcache_check_context(b->device);
+        auto &v = g_bcache.streams[b->device];
+        if (!v.empty()) {
+            b->st = (cudaStream_t)v.back()[0];
+            b->ev_in = (cudaEvent_t)v.back()[1];
+            b->ev_out = (cudaEvent_t)v.back()[2];
+            v.pop_back();
+            return cudaSuccess;
+        }
+    }
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming)) != cudaSuccess)
+        return e;
+    return cudaSuccess;
+}
 
 vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **out)
 {
@@ -2153,11 +2259,9 @@ vfd_status vfd_batch_create(vfd_world *const *worlds, int n_worlds, vfd_batch **
     cudaError_t e = cudaSuccess;
     if ((!oj.empty() && (e = os_prepare()) != cudaSuccess) ||
         ((rfh[0].tiles.size() + rfh[1].tiles.size() + rfh[2].tiles.size()) > 0 && (e = rf_prepare()) != cudaSuccess) ||
-        (e = cudaMalloc(&b->d_arena, ar.host.size())) != cudaSuccess ||
+        (e = take_arena(b->device, ar.host.size(), &b->d_arena)) != cudaSuccess ||
         (e = cudaMemcpy(b->d_arena, ar.host.data(), ar.host.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming)) != cudaSuccess) {
+        (e = take_stream(b)) != cudaSuccess) {
         std::string msg = std::string("batch setup: ") + cudaGetErrorString(e);
         batch_release(b);
         delete b;
