@@ -69,6 +69,7 @@ double latency_of(const vfd_request_info &i) { return i.t_done - i.t_submit; }
 struct Round {
     cudaEvent_t start = nullptr, end = nullptr;
     std::vector<std::shared_ptr<Request>> finishing;  // requests whose last tick this round holds
+    std::vector<vfd_batch *> done_batches;            // batches this round was the last to use
 };
 
 // Worlds are reused by requests of the same shape and parameters.
@@ -274,6 +275,9 @@ void complete_oldest(vfd_server *s)
         s->st.rounds++;
         s->st.device_s += 1e-3 * ms;
     }
+    // a batch the round was the last to use keeps its arena and stream for
+    // the next batch (its work is complete: nothing on the device waits)
+    for (auto *b : rd.done_batches) vfd_batch_destroy(b);
     for (auto &r : rd.finishing) {
         std::string msg;
         const int st = ok ? retire(s, r, msg) : VFD_ERR_CUDA;
@@ -423,8 +427,12 @@ void scheduler(vfd_server *s)
         if (s->active.empty()) continue;
         note_busy(s, true);
         if (s->set_changed || !s->batch) {
-            // the old batch may still be used by rounds in flight: destroyed while idle
-            if (s->batch) s->dead_batches.push_back(s->batch);
+            // the old batch may still be used by rounds in flight: destroyed
+            // when the last of them completes
+            if (s->batch) {
+                if (!s->inflight.empty()) s->inflight.back().done_batches.push_back(s->batch);
+                else vfd_batch_destroy(s->batch);
+            }
             s->batch = nullptr;
             std::vector<vfd_world *> ws;
             for (auto &r : s->active) ws.push_back(r->world);
