@@ -214,6 +214,18 @@ vfd_status vfd_set_spectrum(vfd_world *w, int field, const float *kspec, int fx,
 vfd_status vfd_window_spectrum(const float *window, int kw, int kh, int kd, int cx, int cy, int cz,
                                int fx, int fy, int fz, float *out, int device);
 
+/* The inverse of vfd_window_spectrum: the window (kd*kh*kw floats, x
+ * fastest, centre (cx, cy, cz)) whose wrapped copy has the unscaled R2C
+ * spectrum kspec (host or device, fz*fy*(fx/2+1) interleaved (re, im), the
+ * reference's h_kernelspectrum[ic] layout) on the fx*fy*fz grid, computed on
+ * `device` with this library's inverse transform.  With it a stored spectrum
+ * can be used on any other FFT grid (vfd_set_window): the reference's
+ * power-of-two grid always holds n + window - 1 points per axis, so its
+ * circular convolution is the linear one and the grid can be swapped for
+ * the cheapest one that also avoids wrap-around. */
+vfd_status vfd_spectrum_window(const float *kspec, int fx, int fy, int fz, int kw, int kh, int kd,
+                               int cx, int cy, int cz, float *window, int device);
+
 /* Changes the constant-VF padding of a VFD_METHOD_FFT3D / VFD_METHOD_PLAIN
  * world between ticks: the x bound (the reference passes rightWallIndex =
  * bmcx - 1 to every diffuseChemGPU call, woundHealingWorld.cpp:2407) and,
@@ -429,6 +441,14 @@ vfd_status vfd_write_raw_normalized(const float *field, int nx, int ny, int nz, 
 vfd_status vfd_write_csv(const float *field, int nx, int ny, int nz, const char *path);
 
 /* ---- diagnostics ------------------------------------------------------ */
+/* Exercises the bounded wait the TMA-staged passes use for their bulk copies,
+ * on `device`, against a barrier that no copy will ever complete (none is
+ * issued, so nothing is left in flight): the wait gives up after
+ * limit_cycles SM cycles, records it in the flag the passes use, and this
+ * call returns VFD_ERR_TIMEOUT -- the status vfd_read_mass reports after a
+ * pass's wait gave up.  Any other status means the mechanism is broken. */
+vfd_status vfd_check_wait_timeout(int device, long long limit_cycles);
+
 const char *vfd_status_string(vfd_status s);
 /* Last error message of this world (or of the last failed create when
  * w == NULL, per calling thread).  Never NULL. */

@@ -262,3 +262,17 @@ def test_wide_kernel_uses_full_line_path(gpu, sigma):
     ref = oracle.tick(u, sigma, 0.03, 2, idx, amt)
     assert rel_l2(outs[0], ref) <= REL_L2
     check_mass(outs[0], mass[0], 0.97, 0.0, nx * ny * nz)
+
+
+def test_bounded_wait_reports_timeout(gpu):
+    """Failure detection without a GPU fault: the passes' bounded wait for a
+    bulk copy, run against a barrier that nothing completes, gives up after
+    its limit (2e6 cycles, about 1 ms) and the library reports
+    VFD_ERR_TIMEOUT; the context stays usable (a world ticks afterwards)."""
+    st = vfd.lib().vfd_check_wait_timeout(0, 2_000_000)
+    assert st == 5, vfd.lib().vfd_last_error(None).decode()
+    with vfd.World(32, 24, 16, [vfd.field_params(1.0, 0.1)]) as w:
+        w.upload(0, vfd.synth_field(1, 0, 0, (16, 24, 32)))
+        w.tick(1)
+        m = w.mass()
+        assert m[0]["total"] > 0

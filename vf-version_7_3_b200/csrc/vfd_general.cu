@@ -428,6 +428,25 @@ __global__ void crop_window_kernel(float *w, const float *P, int G, int R, float
     }
 }
 
+// window[z][y][x] = scale * P[(z - cz) mod Fz][(y - cy) mod Fy][(x - cx) mod Fx]:
+// the window whose centre padKernel3D wrapped to index 0, read back from the
+// real grid of an inverse transform.
+__global__ void unwrap_window_kernel(float *w, const float *P, int kw, int kh, int kd, int cx, int cy, int cz,
+                                     int Fx, int Fy, int Fz, float scale)
+{
+    const int64_t n = (int64_t)kw * kh * kd;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % kw);
+        const int64_t r = i / kw;
+        const int y = (int)(r % kh), z = (int)(r / kh);
+        int px = (x - cx) % Fx, py = (y - cy) % Fy, pz = (z - cz) % Fz;
+        if (px < 0) px += Fx;
+        if (py < 0) py += Fy;
+        if (pz < 0) pz += Fz;
+        w[i] = scale * P[(int64_t)px + (int64_t)Fx * (py + (int64_t)Fy * pz)];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Launchers (variant = index into VFD_AXIS_VARIANTS, NL must be 16 for c2c
 // coalescing; any variant works for the row passes).
@@ -567,6 +586,15 @@ cudaError_t launch_crop_window(float *w, const float *P, int G, int R, float sca
 {
     const int64_t k = 2 * R + 1;
     crop_window_kernel<<<grid_for(k * k * k), 256, 0, st>>>(w, P, G, R, scale);
+    note_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unwrap_window(float *w, const float *P, int kw, int kh, int kd, int cx, int cy, int cz, int Fx,
+                                 int Fy, int Fz, float scale, cudaStream_t st)
+{
+    unwrap_window_kernel<<<grid_for((int64_t)kw * kh * kd), 256, 0, st>>>(w, P, kw, kh, kd, cx, cy, cz, Fx, Fy, Fz,
+                                                                          scale);
     note_launch();
     return cudaGetLastError();
 }

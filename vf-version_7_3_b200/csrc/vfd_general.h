@@ -70,5 +70,7 @@ cudaError_t launch_stencil_spectrum(float2 *K, int G, double lambda, double cent
 cudaError_t launch_crop_window(float *w, const float *P, int G, int R, float scale, cudaStream_t st);
 cudaError_t launch_wrap_window(float *P, const float *w, int kw, int kh, int kd, int cx, int cy, int cz, int Fx,
                                int Fy, int Fz, cudaStream_t st);
+cudaError_t launch_unwrap_window(float *w, const float *P, int kw, int kh, int kd, int cx, int cy, int cz, int Fx,
+                                 int Fy, int Fz, float scale, cudaStream_t st);
 
 }  // namespace vfd

@@ -1133,6 +1133,34 @@ cudaError_t rf_prepare()
     return e;
 }
 
+// The bounded wait of the passes on a barrier that no copy will complete:
+// one warp arms the barrier for 1 KB that never arrives (no copy is issued,
+// so nothing is left in flight), waits `limit` cycles and records the
+// give-up in g_rf_timeout exactly as the passes do.
+__global__ void rf_wait_probe_kernel(long long limit, int *gave_up)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncwarp();
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, 1024);
+    __syncwarp();
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar, 0, limit));
+    if (!ok && threadIdx.x == 0) {
+        atomicExch(&g_rf_timeout, 1);
+        *gave_up = 1;
+    }
+}
+
+cudaError_t rf_wait_probe(long long limit, int *gave_up_device, cudaStream_t st)
+{
+    rf_wait_probe_kernel<<<1, 32, 0, st>>>(limit, gave_up_device);
+    note_launch();
+    return cudaGetLastError();
+}
+
 bool rf_take_timeout()
 {
     int v = 0;

@@ -38,5 +38,8 @@ bool rf_encode_map(const OsJob &j, CUtensorMap *m);
 // Reads and clears the flag a pass sets when a bounded wait for a bulk copy
 // gave up.
 bool rf_take_timeout();
+// Runs the passes' bounded barrier wait against a barrier nothing completes
+// (limit in cycles); sets *gave_up_device and the pass timeout flag.
+cudaError_t rf_wait_probe(long long limit, int *gave_up_device, cudaStream_t st);
 
 }  // namespace vfd

@@ -65,14 +65,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// Waits for phase `parity` of the barrier, at most kTmaWaitCycles; false
+// Waits for phase `parity` of the barrier, at most `limit` cycles; false
 // when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit = kTmaWaitCycles)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > kTmaWaitCycles) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 

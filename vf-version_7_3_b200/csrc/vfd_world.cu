@@ -1120,6 +1120,26 @@ vfd_status vfd_set_window(vfd_world *w, int field, const float *window, int kw, 
     return VFD_OK;
 }
 
+vfd_status vfd_check_wait_timeout(int device, long long limit_cycles)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(nullptr, VFD_ERR_NO_DEVICE, "no device");
+    if (device < 0 || device >= ndev || limit_cycles < 1 || limit_cycles > 4000000000ll)
+        return fail(nullptr, VFD_ERR_INVALID_ARG, "bad device or wait limit");
+    DeviceGuard g(device);
+    int *d = nullptr;
+    int h = 0;
+    cudaError_t e = cudaMalloc(&d, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(d, 0, sizeof(int));
+    if (e == cudaSuccess) e = rf_wait_probe(limit_cycles, d, nullptr);
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(nullptr, VFD_ERR_CUDA, std::string("wait probe: ") + cudaGetErrorString(e));
+    const bool flagged = rf_take_timeout();
+    if (h && flagged) return fail(nullptr, VFD_ERR_TIMEOUT, "the bounded wait gave up and reported it");
+    return fail(nullptr, VFD_ERR_CUDA, "the bounded wait did not report giving up");
+}
+
 vfd_status vfd_window_spectrum(const float *window, int kw, int kh, int kd, int cx, int cy, int cz, int fx, int fy,
                                int fz, float *out, int device)
 {
@@ -1166,6 +1186,76 @@ vfd_status vfd_window_spectrum(const float *window, int kw, int kh, int kd, int 
     }
     vfd_world_destroy(w);
     return st;
+}
+
+vfd_status vfd_spectrum_window(const float *kspec, int fx, int fy, int fz, int kw, int kh, int kd, int cx, int cy,
+                               int cz, float *window, int device)
+{
+    if (!kspec || !window || kw < 1 || kh < 1 || kd < 1 || cx < 0 || cx >= kw || cy < 0 || cy >= kh || cz < 0 ||
+        cz >= kd || kw > fx || kh > fy || kd > fz)
+        return fail(nullptr, VFD_ERR_INVALID_ARG, "bad spectrum grid, window or centre");
+    // a one-field world on the (fx, fy, fz) grid: its plans, twiddles and
+    // kernel variants run the inverse transform
+    vfd_field_params p;
+    memset(&p, 0, sizeof(p));
+    p.sigma[0] = p.sigma[1] = p.sigma[2] = 1.0;
+    p.radius[0] = p.radius[1] = p.radius[2] = 1;
+    vfd_world_desc d;
+    memset(&d, 0, sizeof(d));
+    d.nx = fx - 1;
+    d.ny = fy - 1;
+    d.nz = fz - 1;
+    d.n_fields = 1;
+    d.fields = &p;
+    d.fft[0] = fx;
+    d.fft[1] = fy;
+    d.fft[2] = fz;
+    d.method = VFD_METHOD_FFT3D;
+    vfd_world *w = nullptr;
+    vfd_status st = vfd_world_create(&d, device, &w);
+    if (st != VFD_OK) return st;
+    st = vfd_set_spectrum(w, 0, kspec, fx, fy, fz);
+    if (st != VFD_OK) {
+        g_thread_error = w->err;
+        vfd_world_destroy(w);
+        return st;
+    }
+    DeviceGuard g(w->device);
+    const int64_t np = (int64_t)fx * fy * fz;
+    float *P = nullptr, *dw = nullptr;
+    cudaError_t e = cudaMalloc(&P, sizeof(float) * np);
+    if (e == cudaSuccess) e = cudaMalloc(&dw, sizeof(float) * (int64_t)kw * kh * kd);
+    if (e == cudaSuccess) {
+        // inverse z, inverse y (in place on the stored spectrum), C2R along x
+        float2 *K = w->d_kspec;
+        e = launch_gen_cols(w->gvar[2], col_pass(w, PASS_Z, K, fy, fz, fz, GEN_INVERSE), 0);
+        if (e == cudaSuccess) e = launch_gen_cols(w->gvar[1], col_pass(w, PASS_Y, K, fz, fy, fy, GEN_INVERSE), 0);
+        if (e == cudaSuccess) {
+            GenRowPass rp;
+            memset(&rp, 0, sizeof(rp));
+            rp.plan = w->plan[0];
+            rp.tw = w->d_tw[0];
+            rp.nrows = fy * fz;
+            rp.rows_per_plane = fy;
+            rp.r_s1 = fx;
+            rp.r_s2 = (int64_t)fx * fy;
+            rp.c_s1 = w->Fxh;
+            rp.c_s2 = (int64_t)w->Fxh * fy;
+            rp.nstore = fx;
+            rp.rdst = P;
+            rp.csrc = K;
+            e = launch_gen_rows(w->gvar[0], rp, true, 0);
+        }
+        if (e == cudaSuccess)
+            e = launch_unwrap_window(dw, P, kw, kh, kd, cx, cy, cz, fx, fy, fz, (float)(1.0 / (double)np), 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(window, dw, sizeof(float) * (int64_t)kw * kh * kd, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(P);
+    cudaFree(dw);
+    vfd_world_destroy(w);
+    if (e != cudaSuccess) return fail(nullptr, VFD_ERR_CUDA, std::string("spectrum window: ") + cudaGetErrorString(e));
+    return VFD_OK;
 }
 
 vfd_status vfd_set_spectrum(vfd_world *w, int field, const float *kspec, int fx, int fy, int fz)

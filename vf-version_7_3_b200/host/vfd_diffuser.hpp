@@ -17,10 +17,16 @@
 // on only as chem_cctx->h_kernelspectrum[ic], one buffer per chemical
 // (DiffusionHelper.cpp:556-592), filled by computeKernelSpectrum3D
 // (Diffusion.cu:1540-1610): the unscaled R2C spectrum of the wrapped window
-// on the FFTD x FFTH x (FFTW/2+1) grid.  The constructor copies those spectra
-// to the device (vfd_set_spectrum) on a world with the reference's own FFT
-// grid, so the transform the shim runs is the reference's
-// (fftDiffuse3D, Diffusion.cu:1622-1934) with the same spectrum.
+// on the FFTD x FFTH x (FFTW/2+1) grid.  The reference sizes that grid to at
+// least n + window - 1 per axis (DiffusionHelper.cpp:410-437), so its
+// circular convolution is the linear one, and any grid that also avoids
+// wrap-around gives the same result.  The constructor therefore recovers
+// each chemical's window from its spectrum (vfd_spectrum_window, this
+// library's inverse transform) and runs on the cheapest 7-smooth grid of
+// at least n + half-width points per axis (4.3x fewer points than the
+// power-of-two grid at 512x256x384).  With the environment variable
+// VFD_SHIM_REFERENCE_GRID=1 it keeps the reference's grid and uses the
+// spectra as they are (vfd_set_spectrum).
 //
 // Members read, all at construction (the names the reference already uses):
 //   c_ctx:      DW DH DD (data dims), FFTW FFTH FFTD (FFT grid), KW KH KD,
@@ -43,6 +49,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -140,6 +147,8 @@ class DiffuserShim {
                 f.decay_rate = 0.0;
                 f.baseline = whChem_->pbaseline ? whChem_->pbaseline[g.chems[k]] : 0.0f;
             }
+            const char *keep = std::getenv("VFD_SHIM_REFERENCE_GRID");
+            const bool ref_grid = keep && keep[0] == '1';
             vfd_world_desc d;
             d.nx = nx;
             d.ny = ny;
@@ -148,9 +157,9 @@ class DiffuserShim {
             d.fields = p.data();
             d.pad_mode = VFD_PAD_CONSTANT_VF;
             d.epi_boundary = nx;  // replaced by rightWallIndex on every call
-            d.fft[0] = chem_->FFTW;
-            d.fft[1] = chem_->FFTH;
-            d.fft[2] = chem_->FFTD;
+            d.fft[0] = ref_grid ? chem_->FFTW : 0;
+            d.fft[1] = ref_grid ? chem_->FFTH : 0;
+            d.fft[2] = ref_grid ? chem_->FFTD : 0;
             d.method = VFD_METHOD_FFT3D;
             vfd_status s = vfd_world_create(&d, g.device, &g.world);
             if (s != VFD_OK) {
@@ -158,12 +167,22 @@ class DiffuserShim {
                 fail(s, vfd_last_error(nullptr));
                 return;
             }
+            const int kw = chem_->KW, kh = chem_->KH, kd = chem_->KD;
+            std::vector<float> win(ref_grid ? 0 : (size_t)kw * kh * kd);
             for (size_t k = 0; k < g.chems.size(); ++k) {
                 const int ic = g.chems[k];
                 const float *spec = reinterpret_cast<const float *>(chem_->h_kernelspectrum[ic]);
-                s = vfd_set_spectrum(g.world, (int)k, spec, chem_->FFTW, chem_->FFTH, chem_->FFTD);
+                if (ref_grid) {
+                    s = vfd_set_spectrum(g.world, (int)k, spec, chem_->FFTW, chem_->FFTH, chem_->FFTD);
+                } else {
+                    s = vfd_spectrum_window(spec, chem_->FFTW, chem_->FFTH, chem_->FFTD, kw, kh, kd, chem_->KX,
+                                            chem_->KY, chem_->KZ, win.data(), g.device);
+                    if (s == VFD_OK)
+                        s = vfd_set_window(g.world, (int)k, win.data(), kw, kh, kd, chem_->KX, chem_->KY, chem_->KZ);
+                }
                 if (s != VFD_OK) {
-                    fail(s, vfd_last_error(g.world));
+                    fail(s, vfd_last_error(ref_grid ? g.world : nullptr));
+                    if (std::string(err_).empty()) fail(s, vfd_last_error(g.world));
                     return;
                 }
             }

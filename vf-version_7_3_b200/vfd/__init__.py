@@ -47,6 +47,7 @@ EXPORTED = [
     "vfd_autotune", "vfd_world_tuning", "vfd_autotune_set", "vfd_autotune_clear",
     "vfd_set_spectrum", "vfd_set_boundary", "vfd_tick_update", "vfd_diffuse_update_host",
     "vfd_batch_autotune", "vfd_window_spectrum", "vfd_write_raw_normalized", "vfd_write_csv",
+    "vfd_check_wait_timeout", "vfd_spectrum_window",
 ]
 
 PASS_METHODS = {0: "register_fft", 1: "overlap_save", 2: "full_line"}
@@ -142,6 +143,7 @@ def load(path=LIB_PATH):
     lib.vfd_set_window.argtypes = [P, C.c_int, P] + [C.c_int] * 6
     lib.vfd_set_spectrum.argtypes = [P, C.c_int, P, C.c_int, C.c_int, C.c_int]
     lib.vfd_window_spectrum.argtypes = [P] + [C.c_int] * 9 + [P, C.c_int]
+    lib.vfd_spectrum_window.argtypes = [P] + [C.c_int] * 9 + [P, C.c_int]
     lib.vfd_set_boundary.argtypes = [P, C.c_int, P]
     lib.vfd_tick_update.argtypes = [P, C.c_int, C.POINTER(P), P, P]
     lib.vfd_diffuse_update_host.argtypes = [P, C.POINTER(P), C.POINTER(P), P, C.c_int]
@@ -157,6 +159,7 @@ def load(path=LIB_PATH):
     lib.vfd_write_vtk.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_char_p]
     lib.vfd_write_raw_normalized.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_int]
     lib.vfd_write_csv.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_char_p]
+    lib.vfd_check_wait_timeout.argtypes = [C.c_int, C.c_longlong]
     lib.vfd_stencil_window.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, P, C.c_int]
     lib.vfd_synth_field_device.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_float, C.c_float, P,
                                            C.c_size_t, P]
@@ -509,6 +512,18 @@ def write_csv(field, path):
     a = np.ascontiguousarray(field, np.float32)
     nz, ny, nx = a.shape
     _check(lib().vfd_write_csv(_ptr(a), nx, ny, nz, str(path).encode()))
+
+
+def spectrum_window(spec, fx, window_shape, centre=None, device=0):
+    """The window (kd, kh, kw) whose wrapped copy has the R2C spectrum spec
+    (complex (Fz, Fy, Fx/2 + 1)) on the fx x Fy x Fz grid."""
+    a = np.ascontiguousarray(spec, dtype=np.complex64)
+    fz, fy, _ = a.shape
+    kd, kh, kw = window_shape
+    cz, cy, cx = centre if centre is not None else (kd // 2, kh // 2, kw // 2)
+    out = np.empty((kd, kh, kw), np.float32)
+    _check(lib().vfd_spectrum_window(_ptr(a), fx, fy, fz, kw, kh, kd, cx, cy, cz, _ptr(out), device))
+    return out
 
 
 def stencil_window(lam, gamma_dt, n_steps, R, device=0):
