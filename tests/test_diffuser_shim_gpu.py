@@ -75,10 +75,14 @@ def _run(nx, ny, nz, wins, k, fft, base, ins, epi, calls, decay=None, dins=None,
 
 
 @pytest.mark.skipif(not os.path.exists(SHIM), reason="oracle/_ref/libref_shim.so not built (no reference tree)")
-def test_diffuser_dropin_with_reference_cctx(gpu):
+@pytest.mark.parametrize("reference_grid", [False, True])
+def test_diffuser_dropin_with_reference_cctx(gpu, reference_grid, monkeypatch):
     """diffuseChemGPU x2 on 8 chemicals: each equals the reference's own
     kernels + cuFFT with that chemical's spectrum (not another chemical's
-    window, and not the freed kernel context's)."""
+    window, and not the freed kernel context's); on the cheapest grid with
+    the windows recovered from the spectra (default) and on the reference's
+    own grid (VFD_SHIM_REFERENCE_GRID=1)."""
+    monkeypatch.setenv("VFD_SHIM_REFERENCE_GRID", "1" if reference_grid else "0")
     nx, ny, nz, R = 40, 34, 28, 6
     epi = 33
     k, wins, fft, base, ins = _setup(nx, ny, nz, R, 12)

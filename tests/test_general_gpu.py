@@ -311,3 +311,18 @@ def test_against_reference_kernels_on_the_human_scale_grid(gpu):
     e_g3 = rel_l2(g3, ref)
     print(f"config-1 grid vs the reference's kernels + cuFFT: separable {e_sep:.3e}, general {e_g3:.3e}")
     assert e_sep <= REL_L2 and e_g3 <= REL_L2
+
+
+@pytest.mark.parametrize("fft,R", [((64, 48, 56), 6), ((128, 96, 80), 9)])
+def test_spectrum_window_round_trip(gpu, fft, R):
+    """vfd_spectrum_window inverts vfd_window_spectrum: the stencil window
+    comes back from its wrapped spectrum (the drop-in recovers each
+    chemical's window from the reference's stored spectrum this way)."""
+    win = oracle.stencil_power(0.1, 0.0, 2 * R, R).astype(np.float32)
+    spec = vfd.window_spectrum(win, fft)
+    back = vfd.spectrum_window(spec, fft[0], win.shape)
+    assert float(np.abs(back - win).max()) <= 1e-6 * float(win.max())
+    # and from a spectrum made outside the library (numpy, FP64 then FP32)
+    spec_np = _wrapped_spectrum(win, (R, R, R), fft)
+    back2 = vfd.spectrum_window(spec_np, fft[0], win.shape)
+    assert float(np.abs(back2 - win).max()) <= 1e-6 * float(win.max())
