@@ -39,10 +39,11 @@ for p in (os.path.join(ROOT, "vf-version_7_3_b200"), ROOT):
         sys.path.insert(0, p)
 
 METRIC = "voxel-steps/s"
-# ncu dram__bytes_read.sum + dram__bytes_write.sum per axis-pass launch of
-# the human-scale world (8 fields of 512x256x384), scaled by voxels (x 3)
-# from the 512x256x128 capture in profiles/rf_tma_pass_512x256x128.md.
-AXIS_TRAFFIC_BYTES = 3.11e9
+# ncu dram__bytes_read.sum + dram__bytes_write.sum per axis-pass launch,
+# averaged over x, y, z (10.89 GB per launch on the 8 x 768x384x576 world,
+# profiles/rf_tma_pass_512x256x128.md), scaled to the human-scale world by
+# its voxel count (the passes read and write every voxel once).
+AXIS_TRAFFIC_BYTES = 3.23e9
 
 # The configurations, written out here so that the reference arm and the CPU
 # sample need no import of the product package (vfd/configs.py holds the
