@@ -51,6 +51,29 @@ def test_gaussian_general_methods_against_oracle(gpu, method, grid):
 
 
 @pytest.mark.parametrize("method", [vfd.METHOD_FFT3D, vfd.METHOD_PLAIN])
+@pytest.mark.parametrize("fft", [(42, 27, 21), (64, 30, 25), (56, 28, 18), (60, 35, 24), (686, 32, 20)])
+def test_fft_length_splits_against_oracle(gpu, method, fft):
+    """FFT lengths that the register engine splits as F = f1 * f2 with odd
+    and even f2 (42 = 6 x 7, 27 = 3 x 9, 64 = 8 x 8, 30 = 5 x 6, 56 = 7 x 8,
+    28 = 4 x 7, 18 = 3 x 6, 60 = 6 x 10, 35 = 5 x 7, 24 = 4 x 6, 32 = 4 x 8,
+    20 = 4 x 5), and 686 = 2 x 7^3, which has no split with both factors
+    <= 32 and runs on the Stockham stages: one tick against the FP64 oracle,
+    both the fused (FFT3D) and the unfused (PLAIN: forward-only and
+    inverse-only column passes) order."""
+    grid = (37, 20, 13)
+    sig = [1.2, (0.7, 1.4, 1.0)]
+    dec = [0.05, 0.02]
+    ins = configs.field_inputs(0, 3, grid, 100, n_fields=2)
+    outs, mass, dims = run(method, grid, sig, dec, ins, substeps=2, fft=fft)
+    assert tuple(dims) == fft
+    for f, (u, idx, amt) in enumerate(ins):
+        ref = oracle.tick(u, sig[f], dec[f], 2, idx, amt)
+        assert rel_l2(outs[f], ref) <= REL_L2, (method, fft, f, rel_l2(outs[f], ref))
+        s = outs[f].astype(np.float64).sum()
+        assert abs(mass[f]["total"] - s) <= 1e-6 * s
+
+
+@pytest.mark.parametrize("method", [vfd.METHOD_FFT3D, vfd.METHOD_PLAIN])
 def test_constant_vf_general_methods(gpu, method):
     grid = (48, 40, 36)
     nx, ny, nz = grid

@@ -23,15 +23,32 @@
 //   pad_kernel, modulate_kernel, crop_kernel: the unfused elementwise steps.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
 
 #include "vfd_general.h"
 #include "vfd_internal.h"
 
 namespace vfd {
 
-// Global loads each thread keeps in flight before their shared-memory
-// stores in the load loops (the loops are otherwise bound by load latency).
-constexpr int kGU = 6;
+// Tiles are fetched with cp.async: every element of a tile is in flight at
+// once without holding registers (the loads are otherwise bound by latency
+// at the one or two CTAs per SM that the FFT tiles allow).  The issuing
+// thread sees its own copies after cp.async.wait_group, so a pass that
+// touches only the elements it fetched needs no barrier.
+__device__ __forceinline__ void g_cp4(float *smem, const float *gmem, bool valid)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void g_cp8(float2 *smem, const float2 *gmem, bool valid)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void g_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void g_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 __device__ __forceinline__ double warp_sum_g(double v)
 {
@@ -40,7 +57,8 @@ __device__ __forceinline__ double warp_sum_g(double v)
     return v;
 }
 
-template <int NT>
+// Sum of v over the block added to *dst (skipped when dst is NULL or the
+// sum is zero); red holds one double per warp.
 __device__ __forceinline__ void block_sum_atomic_g(double v, double *dst, double *red)
 {
     v = warp_sum_g(v);
@@ -48,39 +66,45 @@ __device__ __forceinline__ void block_sum_atomic_g(double v, double *dst, double
     if (l == 0) red[w] = v;
     __syncthreads();
     if (w == 0) {
-        v = (l < NT / 32) ? red[l] : 0.0;
+        v = (l < (int)(blockDim.x >> 5)) ? red[l] : 0.0;
         v = warp_sum_g(v);
         if (l == 0 && v != 0.0 && dst) atomicAdd(dst, v);
     }
     __syncthreads();
 }
 
-// Shared layout of every general kernel: tile S[F][NL+1] (float2), then F twiddles.
-template <int NL>
-__device__ __forceinline__ void load_twiddles(float2 *tw, const float2 *src, int F, int NT)
+// Shared layout of the Stockham row and column kernels: the tile (F
+// positions of NL + 1 complex values), the F twiddles, then the c2r side
+// buffer [2][NL] or the fused z pass's spectrum tile [F][NL] (when staged).
+// These kernels serve the lengths the register engine (vfd_gen_tpr.cu)
+// cannot split.
+__host__ __device__ __forceinline__ int tile_elems(int F, int NL) { return F * (NL + 1); }
+__device__ __forceinline__ void load_twiddles(float2 *tw, const float2 *src, int F)
 {
-    for (int i = threadIdx.x; i < F; i += NT) tw[i] = src[i];
+    for (int i = threadIdx.x; i < F; i += blockDim.x) tw[i] = src[i];
 }
 
 // ---------------------------------------------------------------------------
+// R2C along x: 2 NL real rows per CTA, rows r0 + l (real parts) and
+// r0 + NL + l (imaginary parts) of complex line l.
 template <int NL, int TL, int MAXP, int MINB>
 __global__ void __launch_bounds__(NL *TL, MINB) r2c_x_kernel(const GenRowPass p)
 {
-    constexpr int NT = NL * TL, LS = NL + 1, NR = 2 * NL;
+    constexpr int NT = NL * TL, NW = NT / 32, LS = NL + 1, NR = 2 * NL;
     extern __shared__ __align__(16) float2 gsm[];
-    __shared__ double red[NT / 32];
+    __shared__ double red[32];
     const int F = p.plan.F;
     float2 *S = gsm;
     float *Sf = reinterpret_cast<float *>(gsm);
-    float2 *tw = S + F * LS;
-    load_twiddles<NL>(tw, p.tw, F, NT);
-
-    const int r0 = blockIdx.x * NR;
-    // real rows: warp w takes tile rows w, w + NT/32, ...; its lanes walk the
-    // row's positions, so every load instruction reads 128 contiguous bytes
+    float2 *tw = S + tile_elems(F, NL);
+    load_twiddles(tw, p.tw, F);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double acc = 0.0;
-    for (int q = warp; q < NR; q += NT / 32) {
+    const int r0 = blockIdx.x * NR;
+
+    // real rows: warp w takes tile rows w, w + NW, ...; its lanes walk the
+    // row's positions (128 contiguous bytes per load); positions >= nload
+    // and rows outside the padding box are zero-filled
+    for (int q = warp; q < NR; q += NW) {
         const int row = r0 + q;
         const int sidx = 2 * (q % NL) + q / NL;
         const bool ok = row < p.nrows;
@@ -93,106 +117,112 @@ __global__ void __launch_bounds__(NL *TL, MINB) r2c_x_kernel(const GenRowPass p)
         if (ok && p.fuse_pad)
             rowin = r1 >= p.box_lo[1] && r1 < p.box_hi[1] && r2 >= p.box_lo[2] && r2 < p.box_hi[2];
         const float *src = p.rsrc + (int64_t)r1 * p.r_s1 + (int64_t)r2 * p.r_s2;
-        // kGU loads in flight per lane before their shared-memory stores
-        for (int x0 = lane; x0 < p.nload; x0 += 32 * kGU) {
-            float v[kGU];
-#pragma unroll
-            for (int u = 0; u < kGU; ++u) {
-                const int x = x0 + 32 * u;
-                v[u] = (rowin && x < p.nload) ? __ldg(src + x) : 0.0f;
+        for (int x = lane; x < F; x += 32) {
+            const bool v = rowin && x < p.nload;
+            g_cp4(&Sf[x * 2 * LS + sidx], v ? src + x : p.rsrc, v);
+        }
+    }
+    g_commit();
+    g_wait<0>();
+    // padding rule and input mass over this thread's own elements
+    double acc = 0.0;
+    if (p.fuse_pad || p.mass_in) {
+        for (int q = warp; q < NR; q += NW) {
+            const int row = r0 + q;
+            const int sidx = 2 * (q % NL) + q / NL;
+            bool rowin = row < p.nrows;
+            if (rowin && p.fuse_pad) {
+                const int r1 = row % p.rows_per_plane, r2 = row / p.rows_per_plane;
+                rowin = r1 >= p.box_lo[1] && r1 < p.box_hi[1] && r2 >= p.box_lo[2] && r2 < p.box_hi[2];
             }
-#pragma unroll
-            for (int u = 0; u < kGU; ++u) {
-                const int x = x0 + 32 * u;
-                if (x < p.nload) {
-                    float w = v[u];
-                    if (p.fuse_pad) w = (rowin && x >= p.box_lo[0] && x < p.box_hi[0]) ? w - p.b : 0.0f;
+            for (int x = lane; x < p.nload; x += 32) {
+                float w = Sf[x * 2 * LS + sidx];
+                if (p.fuse_pad) {
+                    w = (rowin && x >= p.box_lo[0] && x < p.box_hi[0]) ? w - p.b : 0.0f;
                     Sf[x * 2 * LS + sidx] = w;
-                    acc += (double)w;
                 }
+                acc += (double)w;
             }
         }
     }
-    for (int i = p.nload * LS + threadIdx.x; i < F * LS; i += NT) S[i] = make_float2(0.f, 0.f);
     __syncthreads();
     fft_lines<MAXP, TL, NL, false>(S, p.plan, threadIdx.x % NL, threadIdx.x / NL, tw);
 
-    // split the two real rows' half spectra; lanes along k for coalesced rows
+    // split the two real rows' half spectra: warp per output row, lanes along k
     const int Fh = F / 2 + 1;
-    for (int i = threadIdx.x; i < NR * Fh; i += NT) {
-        const int q = i / Fh, k = i - q * Fh;
+    for (int q = warp; q < NR; q += NW) {
         const int rr = r0 + q;
         if (rr >= p.nrows) continue;
         const int ln = q % NL;
-        const float2 z = S[k * LS + ln];
-        const float2 zc = S[((F - k) % F) * LS + ln];  // Z(-k)
-        float2 o;
-        if (q < NL) o = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));       // A(k)
-        else o = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));              // B(k)
         const int s1 = rr % p.rows_per_plane, s2 = rr / p.rows_per_plane;
-        p.cdst[(int64_t)s1 * p.c_s1 + (int64_t)s2 * p.c_s2 + k] = o;
+        float2 *dst = p.cdst + (int64_t)s1 * p.c_s1 + (int64_t)s2 * p.c_s2;
+        for (int k = lane; k < Fh; k += 32) {
+            const float2 z = S[k * LS + ln];
+            const float2 zc = S[(k == 0 ? 0 : F - k) * LS + ln];  // Z(-k)
+            dst[k] = q < NL ? make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y))    // A(k)
+                            : make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));  // B(k)
+        }
     }
-    block_sum_atomic_g<NT>(acc, p.mass_in, red);
+    block_sum_atomic_g(acc, p.mass_in, red);
 }
 
-// ---------------------------------------------------------------------------
+// C2R along x with the optional crop / update epilogue.
 template <int NL, int TL, int MAXP, int MINB>
 __global__ void __launch_bounds__(NL *TL, MINB) c2r_x_kernel(const GenRowPass p)
 {
-    constexpr int NT = NL * TL, LS = NL + 1, NR = 2 * NL;
+    constexpr int NT = NL * TL, NW = NT / 32, LS = NL + 1, NR = 2 * NL;
     extern __shared__ __align__(16) float2 gsm[];
-    __shared__ double red[NT / 32];
+    __shared__ double red[32];
     const int F = p.plan.F;
     const int Fh = F / 2 + 1;
     float2 *S = gsm;
-    float *Sf = reinterpret_cast<float *>(gsm);
-    float2 *tw = S + F * LS;
-    load_twiddles<NL>(tw, p.tw, F, NT);
-
+    const float *Sf = reinterpret_cast<const float *>(gsm);
+    float2 *tw = S + tile_elems(F, NL);
+    float2 *Sb = tw + F;  // [2][NL]
+    load_twiddles(tw, p.tw, F);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r0 = blockIdx.x * NR;
-    // rebuild z(k) = A(k) + i B(k) for every k from the Hermitian halves:
-    // warp w takes line pairs w, w + NT/32, ...; its lanes walk k with kGU
-    // loads of each row in flight
-    {
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        for (int ln = warp; ln < NL; ln += NT / 32) {
-            const int ra = r0 + ln, rb = r0 + NL + ln;
-            const float2 *pa = nullptr, *pb = nullptr;
-            if (ra < p.nrows)
-                pa = p.csrc + (int64_t)(ra % p.rows_per_plane) * p.c_s1 + (int64_t)(ra / p.rows_per_plane) * p.c_s2;
-            if (rb < p.nrows)
-                pb = p.csrc + (int64_t)(rb % p.rows_per_plane) * p.c_s1 + (int64_t)(rb / p.rows_per_plane) * p.c_s2;
-            for (int k0 = lane; k0 < Fh; k0 += 32 * kGU) {
-                float2 A[kGU], B[kGU];
-#pragma unroll
-                for (int u = 0; u < kGU; ++u) {
-                    const int k = k0 + 32 * u;
-                    A[u] = (pa && k < Fh) ? pa[k] : make_float2(0.f, 0.f);
-                    B[u] = (pb && k < Fh) ? pb[k] : make_float2(0.f, 0.f);
-                }
-#pragma unroll
-                for (int u = 0; u < kGU; ++u) {
-                    const int k = k0 + 32 * u;
-                    if (k < Fh) {
-                        // z(k) = A + iB ; z(-k) = conj(A) + i conj(B)
-                        S[k * LS + ln] = make_float2(A[u].x - B[u].y, A[u].y + B[u].x);
-                        if (k > 0 && k < F - k) S[(F - k) * LS + ln] = make_float2(A[u].x + B[u].y, B[u].x - A[u].y);
-                    }
-                }
-            }
+
+    // z(k) = A(k) + i B(k) for every k from the Hermitian halves.  Warp w
+    // takes line pairs w, w + NW, ...; its lanes walk k.  A(k) is fetched
+    // into slot k and B(k) into slot F - k, which z(-k) takes (B(0) and
+    // B(F/2), whose slots A holds, into the side buffer Sb); after the wait
+    // each thread combines the pairs it fetched.
+    for (int ln = warp; ln < NL; ln += NW) {
+        const int ra = r0 + ln, rb = r0 + NL + ln;
+        const float2 *pa = nullptr, *pb = nullptr;
+        if (ra < p.nrows)
+            pa = p.csrc + (int64_t)(ra % p.rows_per_plane) * p.c_s1 + (int64_t)(ra / p.rows_per_plane) * p.c_s2;
+        if (rb < p.nrows)
+            pb = p.csrc + (int64_t)(rb % p.rows_per_plane) * p.c_s1 + (int64_t)(rb / p.rows_per_plane) * p.c_s2;
+        for (int k = lane; k < Fh; k += 32) {
+            float2 *db = k == 0 ? &Sb[ln] : (2 * k == F ? &Sb[NL + ln] : &S[(F - k) * LS + ln]);
+            g_cp8(&S[k * LS + ln], pa ? pa + k : p.csrc, pa != nullptr);
+            g_cp8(db, pb ? pb + k : p.csrc, pb != nullptr);
+        }
+    }
+    g_commit();
+    g_wait<0>();
+    for (int ln = warp; ln < NL; ln += NW) {
+        for (int k = lane; k < Fh; k += 32) {
+            float2 *da = &S[k * LS + ln];
+            float2 *db = k == 0 ? &Sb[ln] : (2 * k == F ? &Sb[NL + ln] : &S[(F - k) * LS + ln]);
+            const float2 A = *da, B = *db;
+            // z(k) = A + iB ; z(-k) = conj(A) + i conj(B)
+            *da = make_float2(A.x - B.y, A.y + B.x);
+            if (k > 0 && k < F - k) *db = make_float2(A.x + B.y, B.x - A.y);
         }
     }
     __syncthreads();
     fft_lines<MAXP, TL, NL, true>(S, p.plan, threadIdx.x % NL, threadIdx.x / NL, tw);
 
     double acc_leak = 0.0, acc_conv = 0.0, acc_out = 0.0;
-    for (int i = threadIdx.x; i < (F - p.nstore) * NL; i += NT) {
-        const float2 x = S[(p.nstore + i / NL) * LS + (i % NL)];
+    for (int j = threadIdx.x; j < (F - p.nstore) * NL; j += NT) {
+        const float2 x = S[(p.nstore + j / NL) * LS + (j % NL)];
         acc_leak += (double)x.x + (double)x.y;
     }
-    // real rows: warp w stores tile rows w, w + NT/32, ...; lanes walk positions
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int q = warp; q < NR; q += NT / 32) {
+    // real rows: warp w stores tile rows w, w + NW, ...; lanes walk positions
+    for (int q = warp; q < NR; q += NW) {
         const int row = r0 + q;
         if (row >= p.nrows) continue;
         const int sidx = 2 * (q % NL) + q / NL;
@@ -201,79 +231,83 @@ __global__ void __launch_bounds__(NL *TL, MINB) c2r_x_kernel(const GenRowPass p)
         // fused WHChemical::update: p = d + decay t, d = 0 (same row layout as the field)
         float *drow = (p.fuse_update && p.dchem) ? p.dchem + (int64_t)r1 * p.r_s1 + (int64_t)r2 * p.r_s2 : nullptr;
         for (int x = lane; x < p.nstore; x += 32) {
-            float t = Sf[x * 2 * LS + sidx];
+            float v = Sf[x * 2 * LS + sidx];
             if (p.fuse_crop) {
-                acc_conv += (double)t;
-                t = p.keep * (t + p.b * p.k0);
+                acc_conv += (double)v;
+                v = p.keep * (v + p.b * p.k0);
                 if (p.fuse_update) {
-                    t *= p.upd_scale;
+                    v *= p.upd_scale;
                     if (drow) {
-                        t += drow[x];
+                        v += drow[x];
                         drow[x] = 0.0f;
                     }
                 }
-                acc_out += (double)t;
+                acc_out += (double)v;
             }
-            dst[x] = t;
+            dst[x] = v;
         }
     }
-    block_sum_atomic_g<NT>(acc_leak, p.mass_leak, red);
-    block_sum_atomic_g<NT>(acc_conv, p.mass_conv, red);
-    block_sum_atomic_g<NT>(acc_out, p.mass_out, red);
+    block_sum_atomic_g(acc_leak, p.mass_leak, red);
+    block_sum_atomic_g(acc_conv, p.mass_conv, red);
+    block_sum_atomic_g(acc_out, p.mass_out, red);
 }
 
-// ---------------------------------------------------------------------------
 // Complex lines: element (line, outer, pos) at base + line + outer*outer_stride
 // + pos*pos_stride (complex units); NL consecutive lines per tile.
 template <int NL, int TL, int MAXP, int MINB>
 __global__ void __launch_bounds__(NL *TL, MINB) c2c_kernel(const GenColPass p)
 {
-    constexpr int NT = NL * TL, LS = NL + 1, NPG = NT / NL;
+    constexpr int NT = NL * TL, LS = NL + 1;
     extern __shared__ __align__(16) float2 gsm[];
     const int F = p.plan.F;
     float2 *S = gsm;
-    float2 *tw = S + F * LS;
-    load_twiddles<NL>(tw, p.tw, F, NT);
+    float2 *tw = S + tile_elems(F, NL);
+    load_twiddles(tw, p.tw, F);
 
     const int tiles_per_outer = (p.nlines + NL - 1) / NL;
     const int outer = blockIdx.x / tiles_per_outer;
     const int l0 = (blockIdx.x - outer * tiles_per_outer) * NL;
+    // thread (ln, pg): line ln of the tile, positions pg, pg + TL, ...
     const int ln = threadIdx.x % NL, pg = threadIdx.x / NL;
     const bool ok = (l0 + ln) < p.nlines;
     float2 *base = p.data + (int64_t)outer * p.outer_stride + l0 + ln;
-    for (int x0 = pg; x0 < p.nload; x0 += NPG * kGU) {
-        float2 v[kGU];
-#pragma unroll
-        for (int u = 0; u < kGU; ++u) {
-            const int x = x0 + NPG * u;
-            v[u] = (ok && x < p.nload) ? base[(int64_t)x * p.pos_stride] : make_float2(0.f, 0.f);
-        }
-#pragma unroll
-        for (int u = 0; u < kGU; ++u) {
-            const int x = x0 + NPG * u;
-            if (x < p.nload) S[x * LS + ln] = v[u];
-        }
+    for (int x = pg; x < F; x += TL) {
+        const bool v = ok && x < p.nload;
+        g_cp8(&S[x * LS + ln], v ? base + (int64_t)x * p.pos_stride : p.data, v);
     }
-    for (int i = p.nload * LS + threadIdx.x; i < F * LS; i += NT) S[i] = make_float2(0.f, 0.f);
+    g_commit();
+    // fused z pass: the spectrum tile K[kz][ky = outer][kx = l0 + l] (F x NL,
+    // after the twiddles) is fetched as a second group, in flight during the
+    // forward transform
+    float2 *Ks = tw + F;
+    const bool ks = p.mode == GEN_FWD_MUL_INV && p.kspec_smem;
+    if (ks) {
+        for (int j = threadIdx.x; j < F * NL; j += NT) {
+            const int k = j / NL, l = j % NL;
+            const bool v = l0 + l < p.nlines;
+            g_cp8(&Ks[j], v ? p.kspec + (int64_t)k * p.k_s_pos + (int64_t)outer * p.k_s_outer + l0 + l : p.kspec, v);
+        }
+        g_commit();
+    }
+    if (ks) g_wait<1>();
+    else g_wait<0>();
     __syncthreads();
     const int line = threadIdx.x % NL, tj = threadIdx.x / NL;
     if (p.mode != GEN_INVERSE) fft_lines<MAXP, TL, NL, false>(S, p.plan, line, tj, tw);
     if (p.mode == GEN_FWD_MUL_INV) {
-        // K[kz][ky][kx]: this tile is ky = outer, kx = l0 + line
-        for (int i = threadIdx.x; i < F * NL; i += NT) {
-            const int k = i / NL, l = i % NL;
-            if (l0 + l < p.nlines) {
-                const float2 kk = p.kspec[(int64_t)k * p.k_s_pos + (int64_t)outer * p.k_s_outer + l0 + l];
-                const float2 x = S[k * LS + l];
-                S[k * LS + l] = make_float2(p.scale * (x.x * kk.x - x.y * kk.y),
-                                            p.scale * (x.x * kk.y + x.y * kk.x));
-            }
+        g_wait<0>();  // this thread's own spectrum elements
+        for (int j = threadIdx.x; j < F * NL; j += NT) {
+            const int k = j / NL, l = j % NL;
+            if (l0 + l >= p.nlines) continue;
+            const float2 kk = ks ? Ks[j] : p.kspec[(int64_t)k * p.k_s_pos + (int64_t)outer * p.k_s_outer + l0 + l];
+            const float2 x = S[k * LS + l];
+            S[k * LS + l] = make_float2(p.scale * (x.x * kk.x - x.y * kk.y), p.scale * (x.x * kk.y + x.y * kk.x));
         }
         __syncthreads();
     }
     if (p.mode != GEN_FORWARD) fft_lines<MAXP, TL, NL, true>(S, p.plan, line, tj, tw);
     if (ok)
-        for (int x = pg; x < p.nstore; x += NPG) base[(int64_t)x * p.pos_stride] = S[x * LS + ln];
+        for (int x = pg; x < p.nstore; x += TL) base[(int64_t)x * p.pos_stride] = S[x * LS + ln];
 }
 
 // ---------------------------------------------------------------------------
@@ -331,8 +365,8 @@ __global__ void crop_kernel(float *u, const float *P, int nx, int ny, int nz, in
         ao += (double)o;
         u[i] = o;
     }
-    block_sum_atomic_g<256>(ac, mass_conv, red);
-    block_sum_atomic_g<256>(ao, mass_out, red);
+    block_sum_atomic_g(ac, mass_conv, red);
+    block_sum_atomic_g(ao, mass_out, red);
 }
 
 // p = d + scale p, d = 0 (d may be NULL): WHChemical::update after a
@@ -350,7 +384,7 @@ __global__ void update_kernel(float *p, float *d, float scale, int64_t n, double
         p[i] = o;
         ao += (double)o;
     }
-    block_sum_atomic_g<256>(ao, mass_out, red);
+    block_sum_atomic_g(ao, mass_out, red);
 }
 
 // Sum of P over the whole FFT grid (the plain path's input mass).
@@ -360,7 +394,7 @@ __global__ void sum_kernel(const float *P, int64_t n, double *out)
     double a = 0.0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         a += (double)P[i];
-    block_sum_atomic_g<256>(a, out, red);
+    block_sum_atomic_g(a, out, red);
 }
 
 // Wrap a window w (kd*kh*kw, centre c) onto the FFT grid so that its centre
@@ -448,8 +482,10 @@ __global__ void unwrap_window_kernel(float *w, const float *P, int kw, int kh, i
 }
 
 // ---------------------------------------------------------------------------
-// Launchers (variant = index into VFD_AXIS_VARIANTS, NL must be 16 for c2c
-// coalescing; any variant works for the row passes).
+// Launchers.  A pass runs on the register engine (vfd_gen_tpr.cu) when its
+// length splits as F = f1 * f2 with f1, f2 <= 32, else on the Stockham kernel
+// variant given (index into VFD_AXIS_VARIANTS; NL 16 for c2c coalescing).
+// VFD_GEN_ENGINE=stockham keeps every pass on the Stockham kernels.
 template <int NL, int TL, int MAXP, int MINB>
 static cudaError_t set_attrs()
 {
@@ -471,7 +507,12 @@ static cudaError_t set_attrs()
     return cudaSuccess;
 }
 
-static size_t gen_smem(int F, int NL) { return (size_t)F * (NL + 1) * sizeof(float2) + (size_t)F * sizeof(float2); }
+// the tile, the twiddles, then the c2r side buffer [2][NL] or the fused z
+// pass's spectrum tile [F][NL]
+static size_t gen_smem(int F, int NL, bool spectrum = false)
+{
+    return ((size_t)tile_elems(F, NL) + F + (spectrum ? (size_t)F * NL : (size_t)2 * NL)) * sizeof(float2);
+}
 
 template <int NL, int TL, int MAXP, int MINB>
 static cudaError_t launch_rows_t(const GenRowPass &p, bool inverse, cudaStream_t st)
@@ -493,13 +534,28 @@ static cudaError_t launch_cols_t(const GenColPass &p, cudaStream_t st)
     if (e != cudaSuccess) return e;
     const int blocks = p.nouter * ((p.nlines + NL - 1) / NL);
     if (blocks <= 0) return cudaSuccess;
-    c2c_kernel<NL, TL, MAXP, MINB><<<blocks, NL * TL, gen_smem(p.plan.F, NL), st>>>(p);
+    // the fused z pass stages its spectrum tile when it fits beside the data
+    GenColPass q = p;
+    q.kspec_smem = p.mode == GEN_FWD_MUL_INV && gen_smem(p.plan.F, NL, true) <= axis_smem_limit();
+    c2c_kernel<NL, TL, MAXP, MINB><<<blocks, NL * TL, gen_smem(p.plan.F, NL, q.kspec_smem != 0), st>>>(q);
     note_launch();
     return cudaGetLastError();
 }
 
+static bool tpr_enabled()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("VFD_GEN_ENGINE");
+        on = !(e && strcmp(e, "stockham") == 0);
+    }
+    return on == 1;
+}
+
 cudaError_t launch_gen_rows(int variant, const GenRowPass &p, bool inverse, cudaStream_t st)
 {
+    const int f1 = tpr_enabled() ? tpr_split(p.plan.F) : 0;
+    if (f1 > 0) return launch_tpr_rows(p, f1, inverse, st);
     switch (variant) {
 #define VFD_GEN_ROW_CASE(i, NL, TL, MAXP, MINB) \
     case i: return launch_rows_t<NL, TL, MAXP, MINB>(p, inverse, st);
@@ -511,6 +567,8 @@ cudaError_t launch_gen_rows(int variant, const GenRowPass &p, bool inverse, cuda
 
 cudaError_t launch_gen_cols(int variant, const GenColPass &p, cudaStream_t st)
 {
+    const int f1 = tpr_enabled() ? tpr_split(p.plan.F) : 0;
+    if (f1 > 0) return launch_tpr_cols(p, f1, st);
     switch (variant) {
 #define VFD_GEN_COL_CASE(i, NL, TL, MAXP, MINB) \
     case i: return launch_cols_t<NL, TL, MAXP, MINB>(p, st);

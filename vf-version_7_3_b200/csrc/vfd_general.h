@@ -51,7 +51,15 @@ struct GenColPass {
     const float2 *kspec;      // GEN_FWD_MUL_INV: spectrum, element (kx, ky, kz) at
     int64_t k_s_outer, k_s_pos;  //   kspec + kx + ky*k_s_outer + kz*k_s_pos
     float scale;
+    int kspec_smem;           // set by the Stockham launcher: spectrum tile staged in shared memory
 };
+
+// Register engine (vfd_gen_tpr.cu).  tpr_split: F = f1 * f2 with
+// f1 <= f2 <= 32 both lengths the engine runs (f2 as small as possible), 0
+// when F has no such split.  The launchers take the split to use.
+int tpr_split(int F);
+cudaError_t launch_tpr_rows(const GenRowPass &p, int f1, bool inverse, cudaStream_t st);
+cudaError_t launch_tpr_cols(const GenColPass &p, int f1, cudaStream_t st);
 
 cudaError_t launch_gen_rows(int variant, const GenRowPass &p, bool inverse, cudaStream_t st);
 cudaError_t launch_gen_cols(int variant, const GenColPass &p, cudaStream_t st);
