@@ -76,14 +76,16 @@ __device__ __forceinline__ TprSmem tpr_smem_layout(float2 *base, int F, int NL)
     m.K = m.Tt + F;
     return m;
 }
-// tw, T and Tt from the global table (no barrier: the caller's follows)
+// tw, T and Tt from the global table (no barrier: the caller's follows).
+// i / d as (i * ceil(2^21 / d)) >> 21, exact for i < 65536 and d <= 32.
 __device__ __forceinline__ void stage_twiddles(const TprSmem &m, const float2 *__restrict__ g, int F, int F1, int F2)
 {
+    const int m1 = ((1 << 21) + F1 - 1) / F1, m2 = ((1 << 21) + F2 - 1) / F2;
     for (int i = threadIdx.x; i < F; i += blockDim.x) {
         m.tw[i] = g[i];
-        const int a = i / F2, b = i - a * F2;  // T: k1 = a, n2 = b
+        const int a = (i * m2) >> 21, b = i - a * F2;  // T: k1 = a, n2 = b
         m.T[i] = g[a * b];
-        const int c = i / F1, d = i - c * F1;  // Tt: n2 = c, k1 = d
+        const int c = (i * m1) >> 21, d = i - c * F1;  // Tt: n2 = c, k1 = d
         m.Tt[i] = g[c * d];
     }
 }
