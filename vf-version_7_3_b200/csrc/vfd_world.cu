@@ -126,6 +126,25 @@ static int choose_fft_len(int n, int r, bool even)
     return best;
 }
 
+// FFT length of a general-method axis: the shortest length >= n + r that the
+// register engine splits into two factors <= 24 (measured on B200 at the
+// 512x256x384 world: x 576 = 24 x 24 runs its row passes in 3.43 ms per tick,
+// 540 = 18 x 30 in 3.98 ms and 560 = 20 x 28 in 4.03 ms), else <= 32, else
+// the Stockham choice.
+static int choose_general_len(int n, int r, bool even)
+{
+    const int lo = n + r;
+    for (int cap : {24, 32}) {
+        for (int F = lo; F <= 2 * lo + 16; ++F) {
+            if (even && (F & 1)) continue;
+            const int f1 = tpr_split(F);
+            FftPlan p;
+            if (f1 > 0 && F / f1 <= cap && make_plan(F, &p) && any_variant_fits(p)) return F;
+        }
+    }
+    return choose_fft_len(n, r, even);
+}
+
 static int pick_variant(const std::vector<FftPlan> &plans, int need_nl = 0)
 {
     static int forced = -2;
@@ -751,7 +770,7 @@ static vfd_status world_create(const vfd_world_desc *d, int device, const ShapeC
             }
             w->plan_order[a] = order;
         } else {
-            F = choose_fft_len(dims[a], rmax[a], general && a == 0);
+            F = general ? choose_general_len(dims[a], rmax[a], a == 0) : choose_fft_len(dims[a], rmax[a], false);
             if (F < 0) {
                 delete w;
                 return fail(nullptr, VFD_ERR_NOT_SUPPORTED, "axis too long for the shared-memory FFT");
