@@ -433,38 +433,52 @@ __global__ void __launch_bounds__(MAXT, MINB) r2c_tpr_kernel(const GenRowPass p,
     tpr_block_sum(acc, p.mass_in, red);
 }
 
-// C2R B' (first pass): bins k1 + F1 k2 of z(k) = A(k) + i B(k) (z(k) =
-// conj A(F-k) + i conj B(F-k) above F/2) loaded, twiddles staged, barrier,
-// inverse DFT F2, times conj w^(n2 k1), slots.
+// C2R B' (first pass).  The half spectra of the tile's 2 NL rows are first
+// fetched with cp.async into the tile's own space as St[q][k] (row q < NL:
+// row a of line q; else row b of line q - NL; Fh bins each): every load is in
+// flight at once without holding registers.  Then thread (k1, l) builds the
+// bins k1 + F1 k2 of z(k) = A(k) + i B(k) (z(k) = conj A(F-k) + i conj B(F-k)
+// above F/2) from St, runs the inverse DFT F2 and the times conj w^(n2 k1)
+// in registers, and after a barrier (St and the slots share the space)
+// writes its slots.
 template <int N, int NL>
 __device__ __forceinline__ void c2r_b(const GenRowPass &p, const TprSmem &m, int r0, int l, int k1, int F1, int GS,
                                       bool active)
 {
-    const int F2 = N, F = F1 * F2, H = F / 2;
+    const int F2 = N, F = F1 * F2, H = F / 2, Fh = H + 1;
+    const int NW = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float2 *St = m.S;
+    for (int q = warp; q < 2 * NL; q += NW) {
+        const RowRef r = row_ref(p, r0 + q, p.c_s1, p.c_s2);
+        const float2 *src = p.csrc + r.off;
+        for (int k = lane; k < Fh; k += 32) tpr_cp8(&St[q * Fh + k], r.ok ? src + k : p.csrc, r.ok);
+    }
+    tpr_cp_commit();
+    stage_twiddles(m, p.tw, F, F1, F2);
+    tpr_cp_wait_all();
+    __syncthreads();
     float2 v[N];
     if (active) {
-        const RowRef ra = row_ref(p, r0 + l, p.c_s1, p.c_s2), rb = row_ref(p, r0 + NL + l, p.c_s1, p.c_s2);
-        const float2 *pa = p.csrc + ra.off, *pb = p.csrc + rb.off;
+        const float2 *sa = St + l * Fh, *sb = St + (NL + l) * Fh;
 #pragma unroll
         for (int k2 = 0; k2 < N; ++k2) {
             const int k = k1 + F1 * k2;
             const bool up = k > H;
             const int kk = up ? F - k : k;
-            const float2 A = ra.ok ? pa[kk] : make_float2(0.f, 0.f);
-            const float2 B = rb.ok ? pb[kk] : make_float2(0.f, 0.f);
+            const float2 A = sa[kk], B = sb[kk];
             v[k2] = up ? make_float2(A.x + B.y, B.x - A.y) : make_float2(A.x - B.y, A.y + B.x);
         }
+        tpr_dft<N, true>(v, m.tw, F1);
+        const float2 *t = m.Tt + k1;  // Tt[n2 F1 + k1], lanes along k1
+#pragma unroll
+        for (int n2 = 1; n2 < N; ++n2) v[n2] = c_conj_mul(v[n2], t[n2 * F1]);
     }
-    stage_twiddles(m, p.tw, F, F1, F2);
     __syncthreads();
-    if (!active) return;
-    tpr_dft<N, true>(v, m.tw, F1);
-    const float2 *t = m.Tt + k1;  // Tt[n2 F1 + k1], lanes along k1
+    if (active) {
+        float2 *grp = m.S + k1 * GS + l;
 #pragma unroll
-    for (int n2 = 1; n2 < N; ++n2) v[n2] = c_conj_mul(v[n2], t[n2 * F1]);
-    float2 *grp = m.S + k1 * GS + l;
-#pragma unroll
-    for (int n2 = 0; n2 < N; ++n2) grp[n2 * (NL + 1)] = v[n2];
+        for (int n2 = 0; n2 < N; ++n2) grp[n2 * (NL + 1)] = v[n2];
+    }
 }
 
 struct C2rSums {
