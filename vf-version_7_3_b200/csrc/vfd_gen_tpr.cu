@@ -98,9 +98,10 @@ __device__ __forceinline__ void tpr_cp8(float2 *smem, const float2 *gmem, bool v
 __device__ __forceinline__ void tpr_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void tpr_cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// Kernels come in two variants: NL = 8 lines per tile with the registers
-// bounded so that 3 CTAs of up to 256 threads stay resident, and NL = 16 with
-// up to 512 threads and one resident CTA.
+// Kernel variants <NL, MAXT, MINB, MAXN>: NL lines per tile, up to MAXT
+// threads, registers bounded for MINB resident CTAs, DFT lengths up to MAXN:
+// <8, 256, 3 or 4, 24> for the lengths the general methods choose, <16, 512,
+// 1, 32> for factors above 24.
 
 // ---------------------------------------------------------------------------
 // Column passes.  Element (line, outer, pos) at data + line + outer *
@@ -219,7 +220,7 @@ __device__ __forceinline__ void col_ai(const GenColPass &p, const TprSmem &m, fl
 
 // One tile = NL consecutive lines of one outer index; thread (l, g) with the
 // line fastest takes group g of each pass.
-template <int NL, int MAXT, int MINB>
+template <int NL, int MAXT, int MINB, int MAXN>
 __global__ void __launch_bounds__(MAXT, MINB) c2c_tpr_kernel(const GenColPass p, int f1)
 {
     constexpr int LS = NL + 1;
@@ -249,7 +250,7 @@ __global__ void __launch_bounds__(MAXT, MINB) c2c_tpr_kernel(const GenColPass p,
     if (p.mode != GEN_INVERSE) {
         switch (F1) {
 #define VFD_COL_A(n) \
-    case n: col_a<n, NL>(p, m, col, g, F2, GS, lok, l, g < F2); break;
+    case n: if constexpr (n <= MAXN) col_a<n, NL>(p, m, col, g, F2, GS, lok, l, g < F2); break;
             VFD_TPR_SIZES(VFD_COL_A)
 #undef VFD_COL_A
         default: break;
@@ -258,7 +259,7 @@ __global__ void __launch_bounds__(MAXT, MINB) c2c_tpr_kernel(const GenColPass p,
         __syncthreads();
         switch (F2) {
 #define VFD_COL_B(n) \
-    case n: col_b<n, NL>(p, m, col, g, F1, GS, lok, l, g < F1); break;
+    case n: if constexpr (n <= MAXN) col_b<n, NL>(p, m, col, g, F1, GS, lok, l, g < F1); break;
             VFD_TPR_SIZES(VFD_COL_B)
 #undef VFD_COL_B
         default: break;
@@ -266,7 +267,7 @@ __global__ void __launch_bounds__(MAXT, MINB) c2c_tpr_kernel(const GenColPass p,
     } else {
         switch (F2) {
 #define VFD_COL_BI(n) \
-    case n: col_bi<n, NL>(p, m, col, g, F1, GS, lok, l, g < F1); break;
+    case n: if constexpr (n <= MAXN) col_bi<n, NL>(p, m, col, g, F1, GS, lok, l, g < F1); break;
             VFD_TPR_SIZES(VFD_COL_BI)
 #undef VFD_COL_BI
         default: break;
@@ -277,7 +278,7 @@ __global__ void __launch_bounds__(MAXT, MINB) c2c_tpr_kernel(const GenColPass p,
         if (g < F2) {
             switch (F1) {
 #define VFD_COL_AI(n) \
-    case n: col_ai<n, NL>(p, m, col, g, F2, GS, lok, l); break;
+    case n: if constexpr (n <= MAXN) col_ai<n, NL>(p, m, col, g, F2, GS, lok, l); break;
                 VFD_TPR_SIZES(VFD_COL_AI)
 #undef VFD_COL_AI
             default: break;
@@ -377,7 +378,7 @@ __device__ __forceinline__ void r2c_b(const TprSmem &m, int l, int k1, int F1, i
     }
 }
 
-template <int NL, int MAXT, int MINB>
+template <int NL, int MAXT, int MINB, int MAXN>
 __global__ void __launch_bounds__(MAXT, MINB) r2c_tpr_kernel(const GenRowPass p, int f1)
 {
     constexpr int LS = NL + 1, NR = 2 * NL;
@@ -394,7 +395,7 @@ __global__ void __launch_bounds__(MAXT, MINB) r2c_tpr_kernel(const GenRowPass p,
         const int n2 = threadIdx.x % F2, l = threadIdx.x / F2;
         switch (F1) {
 #define VFD_R2C_A(n) \
-    case n: acc = r2c_a<n, NL>(p, m, r0, l, n2, F2, GS, l < NL); break;
+    case n: if constexpr (n <= MAXN) acc = r2c_a<n, NL>(p, m, r0, l, n2, F2, GS, l < NL); break;
             VFD_TPR_SIZES(VFD_R2C_A)
 #undef VFD_R2C_A
         default: break;
@@ -406,7 +407,7 @@ __global__ void __launch_bounds__(MAXT, MINB) r2c_tpr_kernel(const GenRowPass p,
         const int l = threadIdx.x % NL, k1 = threadIdx.x / NL;
         switch (F2) {
 #define VFD_R2C_B(n) \
-    case n: r2c_b<n, NL>(m, l, k1, F1, GS, k1 < F1); break;
+    case n: if constexpr (n <= MAXN) r2c_b<n, NL>(m, l, k1, F1, GS, k1 < F1); break;
             VFD_TPR_SIZES(VFD_R2C_B)
 #undef VFD_R2C_B
         default: break;
@@ -530,7 +531,7 @@ __device__ __forceinline__ void c2r_a(const GenRowPass &p, const TprSmem &m, int
     }
 }
 
-template <int NL, int MAXT, int MINB>
+template <int NL, int MAXT, int MINB, int MAXN>
 __global__ void __launch_bounds__(MAXT, MINB) c2r_tpr_kernel(const GenRowPass p, int f1)
 {
     constexpr int NR = 2 * NL;
@@ -545,7 +546,7 @@ __global__ void __launch_bounds__(MAXT, MINB) c2r_tpr_kernel(const GenRowPass p,
         const int k1 = threadIdx.x % F1, l = threadIdx.x / F1;
         switch (F2) {
 #define VFD_C2R_B(n) \
-    case n: c2r_b<n, NL>(p, m, r0, l, k1, F1, GS, l < NL); break;
+    case n: if constexpr (n <= MAXN) c2r_b<n, NL>(p, m, r0, l, k1, F1, GS, l < NL); break;
             VFD_TPR_SIZES(VFD_C2R_B)
 #undef VFD_C2R_B
         default: break;
@@ -559,7 +560,7 @@ __global__ void __launch_bounds__(MAXT, MINB) c2r_tpr_kernel(const GenRowPass p,
         if (l < NL) {
             switch (F1) {
 #define VFD_C2R_A(n) \
-    case n: c2r_a<n, NL>(p, m, r0, l, n2, F2, GS, s); break;
+    case n: if constexpr (n <= MAXN) c2r_a<n, NL>(p, m, r0, l, n2, F2, GS, s); break;
                 VFD_TPR_SIZES(VFD_C2R_A)
 #undef VFD_C2R_A
             default: break;
@@ -619,7 +620,7 @@ static size_t tpr_smem(int F, int NL, bool spectrum)
     return ((size_t)F * (NL + 1) + TPR_MAX + 3 * (size_t)F + (spectrum ? (size_t)F * NL : 0)) * sizeof(float2);
 }
 
-template <int NL, int MAXT, int MINB>
+template <int NL, int MAXT, int MINB, int MAXN>
 static cudaError_t tpr_attrs()
 {
     static thread_local int dev_done = -1;
@@ -627,62 +628,75 @@ static cudaError_t tpr_attrs()
     cudaGetDevice(&dev);
     if (dev_done == dev) return cudaSuccess;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(r2c_tpr_kernel<NL, MAXT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if ((e = cudaFuncSetAttribute(r2c_tpr_kernel<NL, MAXT, MINB, MAXN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)axis_smem_limit())) != cudaSuccess)
         return e;
-    if ((e = cudaFuncSetAttribute(c2r_tpr_kernel<NL, MAXT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if ((e = cudaFuncSetAttribute(c2r_tpr_kernel<NL, MAXT, MINB, MAXN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)axis_smem_limit())) != cudaSuccess)
         return e;
-    if ((e = cudaFuncSetAttribute(c2c_tpr_kernel<NL, MAXT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if ((e = cudaFuncSetAttribute(c2c_tpr_kernel<NL, MAXT, MINB, MAXN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)axis_smem_limit())) != cudaSuccess)
         return e;
     dev_done = dev;
     return cudaSuccess;
 }
 
-template <int NL, int MAXT, int MINB>
+template <int NL, int MAXT, int MINB, int MAXN>
 static cudaError_t rows_nl(const GenRowPass &p, int f1, bool inverse, cudaStream_t st)
 {
-    cudaError_t e = tpr_attrs<NL, MAXT, MINB>();
+    cudaError_t e = tpr_attrs<NL, MAXT, MINB, MAXN>();
     if (e != cudaSuccess) return e;
     const int blocks = (p.nrows + 2 * NL - 1) / (2 * NL);
     if (blocks <= 0) return cudaSuccess;
     const int nt = tpr_threads(p.plan.F, f1, NL);
     const size_t sm = tpr_smem(p.plan.F, NL, false);
     if (nt > MAXT || sm > axis_smem_limit()) return cudaErrorInvalidConfiguration;
-    if (inverse) c2r_tpr_kernel<NL, MAXT, MINB><<<blocks, nt, sm, st>>>(p, f1);
-    else r2c_tpr_kernel<NL, MAXT, MINB><<<blocks, nt, sm, st>>>(p, f1);
+    if (inverse) c2r_tpr_kernel<NL, MAXT, MINB, MAXN><<<blocks, nt, sm, st>>>(p, f1);
+    else r2c_tpr_kernel<NL, MAXT, MINB, MAXN><<<blocks, nt, sm, st>>>(p, f1);
     note_launch();
     return cudaGetLastError();
 }
 
-template <int NL, int MAXT, int MINB>
+template <int NL, int MAXT, int MINB, int MAXN>
 static cudaError_t cols_nl(const GenColPass &p, int f1, cudaStream_t st)
 {
-    cudaError_t e = tpr_attrs<NL, MAXT, MINB>();
+    cudaError_t e = tpr_attrs<NL, MAXT, MINB, MAXN>();
     if (e != cudaSuccess) return e;
     const int64_t blocks = (int64_t)p.nouter * ((p.nlines + NL - 1) / NL);
     if (blocks <= 0) return cudaSuccess;
     const int nt = tpr_threads(p.plan.F, f1, NL);
     const size_t sm = tpr_smem(p.plan.F, NL, p.mode == GEN_FWD_MUL_INV);
     if (nt > MAXT || sm > axis_smem_limit()) return cudaErrorInvalidConfiguration;
-    c2c_tpr_kernel<NL, MAXT, MINB><<<(unsigned)blocks, nt, sm, st>>>(p, f1);
+    c2c_tpr_kernel<NL, MAXT, MINB, MAXN><<<(unsigned)blocks, nt, sm, st>>>(p, f1);
     note_launch();
     return cudaGetLastError();
 }
 
 static bool tpr_split_ok(int F, int f1) { return f1 >= 2 && F % f1 == 0 && tpr_len(f1) && tpr_len(F / f1); }
 
+// the 8-line kernels carry the DFT lengths up to 24 (what the general
+// methods' length choice prefers); longer factors run on the 16-line kernels
+static bool tpr_use16(bool rows, int F, int f1)
+{
+    const int g = f1 > F / f1 ? f1 : F / f1;
+    return tpr_nl(rows) == 16 || g > 24;
+}
+
 cudaError_t launch_tpr_rows(const GenRowPass &p, int f1, bool inverse, cudaStream_t st)
 {
     if (!tpr_split_ok(p.plan.F, f1)) return cudaErrorInvalidValue;
-    return tpr_nl(true) == 16 ? rows_nl<16, 512, 1>(p, f1, inverse, st) : rows_nl<8, 256, 3>(p, f1, inverse, st);
+    if (tpr_use16(true, p.plan.F, f1)) return rows_nl<16, 512, 1, 32>(p, f1, inverse, st);
+    return rows_nl<8, 256, 3, 24>(p, f1, inverse, st);
 }
 
 cudaError_t launch_tpr_cols(const GenColPass &p, int f1, cudaStream_t st)
 {
     if (!tpr_split_ok(p.plan.F, f1)) return cudaErrorInvalidValue;
-    return tpr_nl(false) == 16 ? cols_nl<16, 512, 1>(p, f1, st) : cols_nl<8, 256, 3>(p, f1, st);
+    if (tpr_use16(false, p.plan.F, f1)) return cols_nl<16, 512, 1, 32>(p, f1, st);
+    // measured on B200 (512x256x384 world): the forward-only and inverse-only
+    // passes run best at 4 resident CTAs (64 registers), the fused z pass and
+    // the row passes at 3 (85 registers)
+    return p.mode == GEN_FWD_MUL_INV ? cols_nl<8, 256, 3, 24>(p, f1, st) : cols_nl<8, 256, 4, 24>(p, f1, st);
 }
 
 }  // namespace vfd
