@@ -338,11 +338,23 @@ __device__ __forceinline__ double r2c_a(const GenRowPass &p, const TprSmem &m, i
             }
         }
         if (p.mass_in) {
+            // FP32 pairwise partial sums (error <= ceil(log2 N) ulp of the sum
+            // of magnitudes), widened once
+            float ta[N], tb[N];
 #pragma unroll
             for (int n1 = 0; n1 < N; ++n1) {
-                acc_a += (double)v[n1].x;
-                acc_b += (double)v[n1].y;
+                ta[n1] = v[n1].x;
+                tb[n1] = v[n1].y;
             }
+#pragma unroll
+            for (int w = 1; w < N; w *= 2)
+#pragma unroll
+                for (int i = 0; i + w < N; i += 2 * w) {
+                    ta[i] += ta[i + w];
+                    tb[i] += tb[i + w];
+                }
+            acc_a = (double)ta[0];
+            acc_b = (double)tb[0];
         }
     }
     stage_twiddles(m, p.tw, F, F1, F2);
