@@ -632,31 +632,24 @@ static size_t tpr_smem(int F, int NL, bool spectrum)
     return ((size_t)F * (NL + 1) + TPR_MAX + 3 * (size_t)F + (spectrum ? (size_t)F * NL : 0)) * sizeof(float2);
 }
 
-template <int NL, int MAXT, int MINB, int MAXN>
-static cudaError_t tpr_attrs()
+// The largest dynamic shared memory, once per kernel (one instantiation per
+// kernel, so one flag each) and CUDA context.
+template <auto KERNEL>
+static cudaError_t tpr_attr()
 {
-    static thread_local int dev_done = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev_done == dev) return cudaSuccess;
-    cudaError_t e;
-    if ((e = cudaFuncSetAttribute(r2c_tpr_kernel<NL, MAXT, MINB, MAXN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)axis_smem_limit())) != cudaSuccess)
-        return e;
-    if ((e = cudaFuncSetAttribute(c2r_tpr_kernel<NL, MAXT, MINB, MAXN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)axis_smem_limit())) != cudaSuccess)
-        return e;
-    if ((e = cudaFuncSetAttribute(c2c_tpr_kernel<NL, MAXT, MINB, MAXN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)axis_smem_limit())) != cudaSuccess)
-        return e;
-    dev_done = dev;
-    return cudaSuccess;
+    static thread_local unsigned long long ctx_done = 0;
+    const unsigned long long ctx = current_context_id();
+    if (ctx != 0 && ctx == ctx_done) return cudaSuccess;
+    const cudaError_t e =
+        cudaFuncSetAttribute(KERNEL, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axis_smem_limit());
+    if (e == cudaSuccess) ctx_done = ctx;
+    return e;
 }
 
 template <int NL, int MAXT, int MINB, int MAXN>
 static cudaError_t rows_nl(const GenRowPass &p, int f1, bool inverse, cudaStream_t st)
 {
-    cudaError_t e = tpr_attrs<NL, MAXT, MINB, MAXN>();
+    cudaError_t e = inverse ? tpr_attr<c2r_tpr_kernel<NL, MAXT, MINB, MAXN>>() : tpr_attr<r2c_tpr_kernel<NL, MAXT, MINB, MAXN>>();
     if (e != cudaSuccess) return e;
     const int blocks = (p.nrows + 2 * NL - 1) / (2 * NL);
     if (blocks <= 0) return cudaSuccess;
@@ -672,7 +665,7 @@ static cudaError_t rows_nl(const GenRowPass &p, int f1, bool inverse, cudaStream
 template <int NL, int MAXT, int MINB, int MAXN>
 static cudaError_t cols_nl(const GenColPass &p, int f1, cudaStream_t st)
 {
-    cudaError_t e = tpr_attrs<NL, MAXT, MINB, MAXN>();
+    cudaError_t e = tpr_attr<c2c_tpr_kernel<NL, MAXT, MINB, MAXN>>();
     if (e != cudaSuccess) return e;
     const int64_t blocks = (int64_t)p.nouter * ((p.nlines + NL - 1) / NL);
     if (blocks <= 0) return cudaSuccess;

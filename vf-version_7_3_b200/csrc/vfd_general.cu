@@ -9,6 +9,11 @@
 // The spectrum is laid out [z][y][kx] with Fxh = Fx/2 + 1 bins per row
 // (the reference's fftD x fftH x (fftW/2 + 1), Diffusion.cu:1687).
 //
+// The row and column passes run on the two-pass register FFT
+// (vfd_gen_tpr.cu) when the line length splits as f1 * f2 with f1, f2 <= 32;
+// the Stockham kernels below serve every other length (and all lengths with
+// VFD_GEN_ENGINE=stockham).  launch_gen_rows / launch_gen_cols choose.
+//
 // Kernels:
 //   r2c_x_kernel   real rows -> half spectra.  Two real rows form one complex
 //                  line z = a + i b; after the FFT, A(k) = (Z(k) + conj Z(-k))/2,
@@ -489,10 +494,10 @@ __global__ void unwrap_window_kernel(float *w, const float *P, int kw, int kh, i
 template <int NL, int TL, int MAXP, int MINB>
 static cudaError_t set_attrs()
 {
-    static thread_local int dev_done = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev_done == dev) return cudaSuccess;
+    // once per CUDA context (a device reset starts a new one)
+    static thread_local unsigned long long ctx_done = 0;
+    const unsigned long long ctx = current_context_id();
+    if (ctx != 0 && ctx == ctx_done) return cudaSuccess;
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(r2c_x_kernel<NL, TL, MAXP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)axis_smem_limit())) != cudaSuccess)
@@ -503,7 +508,7 @@ static cudaError_t set_attrs()
     if ((e = cudaFuncSetAttribute(c2c_kernel<NL, TL, MAXP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)axis_smem_limit())) != cudaSuccess)
         return e;
-    dev_done = dev;
+    ctx_done = ctx;
     return cudaSuccess;
 }
 
