@@ -73,6 +73,23 @@ def test_fft_length_splits_against_oracle(gpu, method, fft):
         assert abs(mass[f]["total"] - s) <= 1e-6 * s
 
 
+def test_long_z_line_fused_pass_against_oracle(gpu):
+    """A fused z pass on a 1024-point line (32 x 32, the reference's
+    power-of-two size for 512 < nz + r <= 1024): its 16-line register tile
+    and spectrum tile exceed shared memory, so it runs on the Stockham
+    kernels; the x and y passes stay on the register engine."""
+    grid = (20, 12, 600)
+    sig = [1.1]
+    ins = configs.field_inputs(2, 3, grid, 50, n_fields=1)
+    outs, mass, dims = run(vfd.METHOD_FFT3D, grid, sig, [0.03], ins, substeps=1, fft=(32, 24, 1024))
+    assert tuple(dims) == (32, 24, 1024)
+    u, idx, amt = ins[0]
+    ref = oracle.tick(u, sig[0], 0.03, 1, idx, amt)
+    assert rel_l2(outs[0], ref) <= REL_L2, rel_l2(outs[0], ref)
+    s = outs[0].astype(np.float64).sum()
+    assert abs(mass[0]["total"] - s) <= 1e-6 * s
+
+
 @pytest.mark.parametrize("method", [vfd.METHOD_FFT3D, vfd.METHOD_PLAIN])
 def test_constant_vf_general_methods(gpu, method):
     grid = (48, 40, 36)

@@ -573,7 +573,12 @@ cudaError_t launch_gen_rows(int variant, const GenRowPass &p, bool inverse, cuda
 cudaError_t launch_gen_cols(int variant, const GenColPass &p, cudaStream_t st)
 {
     const int f1 = tpr_enabled() ? tpr_split(p.plan.F) : 0;
-    if (f1 > 0) return launch_tpr_cols(p, f1, st);
+    if (f1 > 0) {
+        // a fused z pass whose tile and spectrum tile do not fit in shared
+        // memory (16-line tiles of long lines) runs on the Stockham kernels
+        const cudaError_t e = launch_tpr_cols(p, f1, st);
+        if (e != cudaErrorInvalidConfiguration) return e;
+    }
     switch (variant) {
 #define VFD_GEN_COL_CASE(i, NL, TL, MAXP, MINB) \
     case i: return launch_cols_t<NL, TL, MAXP, MINB>(p, st);

@@ -56,7 +56,9 @@ struct GenColPass {
 
 // Register engine (vfd_gen_tpr.cu).  tpr_split: F = f1 * f2 with
 // f1 <= f2 <= 32 both lengths the engine runs (f2 as small as possible), 0
-// when F has no such split.  The launchers take the split to use.
+// when F has no such split.  The launchers take the split to use; they
+// return cudaErrorInvalidConfiguration, without launching, when the tile
+// does not fit in shared memory.
 int tpr_split(int F);
 cudaError_t launch_tpr_rows(const GenRowPass &p, int f1, bool inverse, cudaStream_t st);
 cudaError_t launch_tpr_cols(const GenColPass &p, int f1, cudaStream_t st);
