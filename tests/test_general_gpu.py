@@ -75,9 +75,9 @@ def test_fft_length_splits_against_oracle(gpu, method, fft):
 
 def test_long_z_line_fused_pass_against_oracle(gpu):
     """A fused z pass on a 1024-point line (32 x 32, the reference's
-    power-of-two size for 512 < nz + r <= 1024): its 16-line register tile
-    and spectrum tile exceed shared memory, so it runs on the Stockham
-    kernels; the x and y passes stay on the register engine."""
+    power-of-two size for 512 < nz + r <= 1024): the 16-line register
+    kernels with the spectrum read from global memory, next to 8-line x and
+    y passes, against the FP64 oracle."""
     grid = (20, 12, 600)
     sig = [1.1]
     ins = configs.field_inputs(2, 3, grid, 50, n_fields=1)

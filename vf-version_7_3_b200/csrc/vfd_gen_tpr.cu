@@ -22,9 +22,13 @@
 //
 // Shared memory: the tile, then the twiddles tw[m] = w_F^m and the pass
 // twiddles w_F^(k1 n2) in both orders (T[k1 F2 + n2] for lanes along n2,
-// Tt[n2 F1 + k1] for lanes along k1, so that neither gather conflicts), then
-// the fused z pass's spectrum tile [F][NL].  The first pass's global loads
-// are issued before the twiddle staging and its barrier, so they overlap.
+// Tt[n2 F1 + k1] for lanes along k1, so that neither gather conflicts).  The
+// first pass's global loads are issued before the twiddle staging and its
+// barrier, so they overlap.  The fused z pass reads its spectrum K straight
+// from global memory in pass B (lanes along lines: coalesced), which leaves
+// the shared memory to the tile and more CTAs per SM (measured on B200, the
+// 512x256x384 world: 2.23 -> 1.96 ms per tick against staging K by
+// cp.async).
 // Tile: slot n2 + F2 k1 of line l at S[n2 * LS + k1 * GS + l] with
 // LS = NL + 1 and GS = F2 * LS + pad, pad = 1 when F2 is even (an odd GS
 // keeps the walks along k1 free of bank conflicts); the R2C pass B leaves
@@ -64,7 +68,7 @@ __device__ __forceinline__ void tpr_block_sum(double v, double *dst, double *red
 __device__ __forceinline__ float2 c_conj_mul(float2 a, float2 w) { return c_mul(a, make_float2(w.x, -w.y)); }
 
 struct TprSmem {
-    float2 *S, *tw, *T, *Tt, *K;
+    float2 *S, *tw, *T, *Tt;
 };
 __device__ __forceinline__ TprSmem tpr_smem_layout(float2 *base, int F, int NL)
 {
@@ -73,7 +77,6 @@ __device__ __forceinline__ TprSmem tpr_smem_layout(float2 *base, int F, int NL)
     m.tw = base + F * (NL + 1) + TPR_MAX;
     m.T = m.tw + F;
     m.Tt = m.T + F;
-    m.K = m.Tt + F;
     return m;
 }
 // tw, T and Tt from the global table (no barrier: the caller's follows).
@@ -148,10 +151,11 @@ __device__ __forceinline__ void col_b_inverse(const TprSmem &m, float2 (&v)[N], 
 }
 
 // B of group k1 (after A): slots -> DFT F2 -> bins k1 + F1 k2 to global
-// (GEN_FORWARD), or times K/N (the staged spectrum tile) and B'.
+// (GEN_FORWARD), or times K/N (K[kz = bin][ky = outer][kx = l0 + l] from
+// global memory) and B'.
 template <int N, int NL>
 __device__ __forceinline__ void col_b(const GenColPass &p, const TprSmem &m, float2 *col, int k1, int F1, int GS,
-                                      bool lok, int l, bool active)
+                                      bool lok, int l, int outer, int l0, bool active)
 {
     if (!active) return;
     float2 v[N];
@@ -169,10 +173,10 @@ __device__ __forceinline__ void col_b(const GenColPass &p, const TprSmem &m, flo
         }
         return;
     }
-    // times K[kz = bin][ky = outer][kx = l0 + l] (staged as K[bin][l]) and 1/N
+    const float2 *kp = p.kspec + (int64_t)outer * p.k_s_outer + l0 + l;
 #pragma unroll
     for (int k2 = 0; k2 < N; ++k2) {
-        const float2 kk = m.K[(k1 + F1 * k2) * NL + l];
+        const float2 kk = lok ? kp[(int64_t)(k1 + F1 * k2) * p.k_s_pos] : make_float2(0.f, 0.f);
         const float2 x = v[k2];
         v[k2] = make_float2(p.scale * (x.x * kk.x - x.y * kk.y), p.scale * (x.x * kk.y + x.y * kk.x));
     }
@@ -236,17 +240,6 @@ __global__ void __launch_bounds__(MAXT, MINB) c2c_tpr_kernel(const GenColPass p,
     const bool lok = l0 + l < p.nlines;
     float2 *col = p.data + (int64_t)outer * p.outer_stride + l0 + l;
 
-    if (p.mode == GEN_FWD_MUL_INV) {
-        // spectrum tile K[bin][line] of this (ky = outer, kx = l0 ..) column
-        // set, in flight during pass A
-        for (int j = threadIdx.x; j < F * NL; j += blockDim.x) {
-            const int bin = j / NL, ll = j - bin * NL;
-            const bool v = l0 + ll < p.nlines;
-            tpr_cp8(&m.K[j], v ? p.kspec + (int64_t)bin * p.k_s_pos + (int64_t)outer * p.k_s_outer + l0 + ll : p.kspec,
-                    v);
-        }
-        tpr_cp_commit();
-    }
     if (p.mode != GEN_INVERSE) {
         switch (F1) {
 #define VFD_COL_A(n) \
@@ -255,11 +248,10 @@ __global__ void __launch_bounds__(MAXT, MINB) c2c_tpr_kernel(const GenColPass p,
 #undef VFD_COL_A
         default: break;
         }
-        tpr_cp_wait_all();
         __syncthreads();
         switch (F2) {
 #define VFD_COL_B(n) \
-    case n: if constexpr (n <= MAXN) col_b<n, NL>(p, m, col, g, F1, GS, lok, l, g < F1); break;
+    case n: if constexpr (n <= MAXN) col_b<n, NL>(p, m, col, g, F1, GS, lok, l, outer, l0, g < F1); break;
             VFD_TPR_SIZES(VFD_COL_B)
 #undef VFD_COL_B
         default: break;
@@ -626,11 +618,8 @@ static int tpr_threads(int F, int f1, int NL)
     return (NL * g + 31) / 32 * 32;
 }
 
-// the tile, tw, T, Tt, and the fused z pass's spectrum tile
-static size_t tpr_smem(int F, int NL, bool spectrum)
-{
-    return ((size_t)F * (NL + 1) + TPR_MAX + 3 * (size_t)F + (spectrum ? (size_t)F * NL : 0)) * sizeof(float2);
-}
+// the tile, tw, T and Tt
+static size_t tpr_smem(int F, int NL) { return ((size_t)F * (NL + 1) + TPR_MAX + 3 * (size_t)F) * sizeof(float2); }
 
 // The largest dynamic shared memory, once per kernel (one instantiation per
 // kernel, so one flag each) and CUDA context.
@@ -654,7 +643,7 @@ static cudaError_t rows_nl(const GenRowPass &p, int f1, bool inverse, cudaStream
     const int blocks = (p.nrows + 2 * NL - 1) / (2 * NL);
     if (blocks <= 0) return cudaSuccess;
     const int nt = tpr_threads(p.plan.F, f1, NL);
-    const size_t sm = tpr_smem(p.plan.F, NL, false);
+    const size_t sm = tpr_smem(p.plan.F, NL);
     if (nt > MAXT || sm > axis_smem_limit()) return cudaErrorInvalidConfiguration;
     if (inverse) c2r_tpr_kernel<NL, MAXT, MINB, MAXN><<<blocks, nt, sm, st>>>(p, f1);
     else r2c_tpr_kernel<NL, MAXT, MINB, MAXN><<<blocks, nt, sm, st>>>(p, f1);
@@ -670,7 +659,7 @@ static cudaError_t cols_nl(const GenColPass &p, int f1, cudaStream_t st)
     const int64_t blocks = (int64_t)p.nouter * ((p.nlines + NL - 1) / NL);
     if (blocks <= 0) return cudaSuccess;
     const int nt = tpr_threads(p.plan.F, f1, NL);
-    const size_t sm = tpr_smem(p.plan.F, NL, p.mode == GEN_FWD_MUL_INV);
+    const size_t sm = tpr_smem(p.plan.F, NL);
     if (nt > MAXT || sm > axis_smem_limit()) return cudaErrorInvalidConfiguration;
     c2c_tpr_kernel<NL, MAXT, MINB, MAXN><<<(unsigned)blocks, nt, sm, st>>>(p, f1);
     note_launch();

@@ -574,8 +574,8 @@ cudaError_t launch_gen_cols(int variant, const GenColPass &p, cudaStream_t st)
 {
     const int f1 = tpr_enabled() ? tpr_split(p.plan.F) : 0;
     if (f1 > 0) {
-        // a fused z pass whose tile and spectrum tile do not fit in shared
-        // memory (16-line tiles of long lines) runs on the Stockham kernels
+        // a pass whose register-engine tile would not fit in shared memory
+        // runs on the Stockham kernels
         const cudaError_t e = launch_tpr_cols(p, f1, st);
         if (e != cudaErrorInvalidConfiguration) return e;
     }
