@@ -490,11 +490,13 @@ struct C2rSums {
     double leak = 0.0, conv = 0.0, out = 0.0;
 };
 
-// One real output value at x of a row: the crop / update epilogue.
-__device__ __forceinline__ void c2r_store(const GenRowPass &p, float t, float *dst, float *drow, int x, C2rSums &s)
+// One real output value at x of a row: the crop / update epilogue; the
+// values for the mass totals are added to the FP32 group sums gc and go.
+__device__ __forceinline__ void c2r_store(const GenRowPass &p, float t, float *dst, float *drow, int x, float &gc,
+                                          float &go)
 {
     if (p.fuse_crop) {
-        s.conv += (double)t;
+        gc += t;
         t = p.keep * (t + p.b * p.k0);
         if (p.fuse_update) {
             t *= p.upd_scale;
@@ -503,13 +505,15 @@ __device__ __forceinline__ void c2r_store(const GenRowPass &p, float t, float *d
                 drow[x] = 0.0f;
             }
         }
-        s.out += (double)t;
+        go += t;
     }
     dst[x] = t;
 }
 
 // C2R A': slots of group n2 -> inverse DFT F1 -> positions n2 + F2 n1 of rows
-// a (real part) and b (imaginary part); positions >= nstore go to the leak sum.
+// a (real part) and b (imaginary part); positions >= nstore go to the leak
+// sum.  The mass sums run in FP32 over groups of 4 positions, each group
+// widened once into the FP64 totals.
 template <int N, int NL>
 __device__ __forceinline__ void c2r_a(const GenRowPass &p, const TprSmem &m, int r0, int l, int n2, int F2, int GS,
                                       C2rSums &s)
@@ -523,14 +527,21 @@ __device__ __forceinline__ void c2r_a(const GenRowPass &p, const TprSmem &m, int
     float *da = p.rdst + ra.off, *db = p.rdst + rb.off;
     float *ua = (p.fuse_update && p.dchem) ? p.dchem + ra.off : nullptr;
     float *ub = (p.fuse_update && p.dchem) ? p.dchem + rb.off : nullptr;
+    float gc = 0.0f, go = 0.0f, gl = 0.0f;
 #pragma unroll
     for (int n1 = 0; n1 < N; ++n1) {
         const int x = n2 + F2 * n1;
         if (x < p.nstore) {
-            if (ra.ok) c2r_store(p, v[n1].x, da, ua, x, s);
-            if (rb.ok) c2r_store(p, v[n1].y, db, ub, x, s);
+            if (ra.ok) c2r_store(p, v[n1].x, da, ua, x, gc, go);
+            if (rb.ok) c2r_store(p, v[n1].y, db, ub, x, gc, go);
         } else {
-            s.leak += (double)v[n1].x + (double)v[n1].y;
+            gl += v[n1].x + v[n1].y;
+        }
+        if ((n1 & 3) == 3 || n1 == N - 1) {
+            s.conv += (double)gc;
+            s.out += (double)go;
+            s.leak += (double)gl;
+            gc = go = gl = 0.0f;
         }
     }
 }
