@@ -2000,13 +2000,16 @@ vfd_status vfd_diffuse_host(vfd_world *w, const float *const *host_in, float *co
     for (int f = 0; f < w->nf; ++f)
         if (!host_in[f] || !host_out[f]) return fail(w, VFD_ERR_INVALID_ARG, "NULL host buffer");
     DeviceGuard g(w->device);
-    vfd_status s = sync_sources(w, w->s_cmp);
-    if (s != VFD_OK) return s;
+    vfd_status s = VFD_OK;
     const size_t bytes = sizeof(float) * w->V;
     for (int f = 0; f < w->nf; ++f) {
         float *dev = w->d_fields + (int64_t)f * w->V;
         VFD_CUDA(w, cudaMemcpyAsync(dev, host_in[f], bytes, cudaMemcpyHostToDevice, w->s_in));
         VFD_CUDA(w, cudaEventRecord(w->ev_in[f], w->s_in));
+        // the sources go up on the compute stream (ahead of every tick)
+        // while the first field is in flight: their pageable copies hold the
+        // host until staged
+        if (f == 0 && (s = sync_sources(w, w->s_cmp)) != VFD_OK) return s;
         VFD_CUDA(w, cudaStreamWaitEvent(w->s_cmp, w->ev_in[f], 0));
         s = enqueue_tick(w, f, n_substeps, w->s_cmp);
         if (s != VFD_OK) return s;
@@ -2033,8 +2036,7 @@ vfd_status vfd_diffuse_update_host(vfd_world *w, float *const *host_p, float *co
         if (!std::isfinite(decay[f])) return fail(w, VFD_ERR_INVALID_ARG, "decay must be finite");
     }
     DeviceGuard g(w->device);
-    vfd_status s = sync_sources(w, w->s_cmp);
-    if (s != VFD_OK) return s;
+    vfd_status s = VFD_OK;
     const size_t bytes = sizeof(float) * w->V;
     if (host_d && !w->d_upd) VFD_CUDA(w, cudaMalloc(&w->d_upd, bytes * w->nf));
     std::vector<float *> dptr(w->nf, nullptr);
@@ -2045,6 +2047,8 @@ vfd_status vfd_diffuse_update_host(vfd_world *w, float *const *host_p, float *co
         VFD_CUDA(w, cudaMemcpyAsync(dev, host_p[f], bytes, cudaMemcpyHostToDevice, w->s_in));
         if (dptr[f]) VFD_CUDA(w, cudaMemcpyAsync(dptr[f], host_d[f], bytes, cudaMemcpyHostToDevice, w->s_in));
         VFD_CUDA(w, cudaEventRecord(w->ev_in[f], w->s_in));
+        // sources ahead of every tick, staged while the first field is in flight
+        if (f == 0 && (s = sync_sources(w, w->s_cmp)) != VFD_OK) return s;
         VFD_CUDA(w, cudaStreamWaitEvent(w->s_cmp, w->ev_in[f], 0));
         // the update reads decay[f] and dchem[f] only for field f
         const UpdateArgs upd{dptr.data(), decay};
