@@ -20,7 +20,7 @@
 // passes (NL consecutive lines, 128 bytes for NL = 16), positions n2 (the
 // first pass) or bins k1 (the C2R first pass) for the row passes.
 //
-// Shared memory: the tile, then the twiddles tw[m] = w_F^m and the pass
+// Shared memory: the tile, then (unused room for tw[m] = w_F^m) the pass
 // twiddles w_F^(k1 n2) in both orders (T[k1 F2 + n2] for lanes along n2,
 // Tt[n2 F1 + k1] for lanes along k1, so that neither gather conflicts).  The
 // first pass's global loads are issued before the twiddle staging and its
@@ -79,13 +79,13 @@ __device__ __forceinline__ TprSmem tpr_smem_layout(float2 *base, int F, int NL)
     m.Tt = m.T + F;
     return m;
 }
-// tw, T and Tt from the global table (no barrier: the caller's follows).
+// T and Tt from the global table (no barrier: the caller's follows; the
+// small DFTs take their twiddles as immediates, so tw is not staged).
 // i / d as (i * ceil(2^21 / d)) >> 21, exact for i < 65536 and d <= 32.
 __device__ __forceinline__ void stage_twiddles(const TprSmem &m, const float2 *__restrict__ g, int F, int F1, int F2)
 {
     const int m1 = ((1 << 21) + F1 - 1) / F1, m2 = ((1 << 21) + F2 - 1) / F2;
     for (int i = threadIdx.x; i < F; i += blockDim.x) {
-        m.tw[i] = g[i];
         const int a = (i * m2) >> 21, b = i - a * F2;  // T: k1 = a, n2 = b
         m.T[i] = g[a * b];
         const int c = (i * m1) >> 21, d = i - c * F1;  // Tt: n2 = c, k1 = d
@@ -128,7 +128,7 @@ __device__ __forceinline__ void col_a(const GenColPass &p, const TprSmem &m, con
     stage_twiddles(m, p.tw, F, F1, F2);
     __syncthreads();
     if (!active) return;
-    tpr_dft<N, false>(v, m.tw, F2);
+    tpr_dft<N, false>(v);
     const float2 *t = m.T + n2;  // T[k1 F2 + n2]
 #pragma unroll
     for (int k1 = 1; k1 < N; ++k1) v[k1] = c_mul(v[k1], t[k1 * F2]);
@@ -141,7 +141,7 @@ __device__ __forceinline__ void col_a(const GenColPass &p, const TprSmem &m, con
 template <int N, int NL>
 __device__ __forceinline__ void col_b_inverse(const TprSmem &m, float2 (&v)[N], int k1, int F1, int GS, int l)
 {
-    tpr_dft<N, true>(v, m.tw, F1);
+    tpr_dft<N, true>(v);
     const float2 *t = m.T + k1 * N;  // T[k1 F2 + n2]
 #pragma unroll
     for (int n2 = 1; n2 < N; ++n2) v[n2] = c_conj_mul(v[n2], t[n2]);
@@ -162,7 +162,7 @@ __device__ __forceinline__ void col_b(const GenColPass &p, const TprSmem &m, flo
     const float2 *grp = m.S + k1 * GS + l;  // slot F2 k1 + n2 at grp[n2 * LS]
 #pragma unroll
     for (int n2 = 0; n2 < N; ++n2) v[n2] = grp[n2 * (NL + 1)];
-    tpr_dft<N, false>(v, m.tw, F1);
+    tpr_dft<N, false>(v);
     if (p.mode == GEN_FORWARD) {
         if (lok) {
 #pragma unroll
@@ -212,7 +212,7 @@ __device__ __forceinline__ void col_ai(const GenColPass &p, const TprSmem &m, fl
     const float2 *s = m.S + n2 * (NL + 1) + l;
 #pragma unroll
     for (int k1 = 0; k1 < N; ++k1) v[k1] = s[k1 * GS];
-    tpr_dft<N, true>(v, m.tw, F2);
+    tpr_dft<N, true>(v);
     if (lok) {
 #pragma unroll
         for (int n1 = 0; n1 < N; ++n1) {
@@ -352,7 +352,7 @@ __device__ __forceinline__ double r2c_a(const GenRowPass &p, const TprSmem &m, i
     stage_twiddles(m, p.tw, F, F1, F2);
     __syncthreads();
     if (active) {
-        tpr_dft<N, false>(v, m.tw, F2);
+        tpr_dft<N, false>(v);
         const float2 *t = m.T + n2;  // T[k1 F2 + n2], lanes along n2
 #pragma unroll
         for (int k1 = 1; k1 < N; ++k1) v[k1] = c_mul(v[k1], t[k1 * F2]);
@@ -373,7 +373,7 @@ __device__ __forceinline__ void r2c_b(const TprSmem &m, int l, int k1, int F1, i
         const float2 *grp = m.S + k1 * GS + l;
 #pragma unroll
         for (int n2 = 0; n2 < N; ++n2) v[n2] = grp[n2 * (NL + 1)];
-        tpr_dft<N, false>(v, m.tw, F1);
+        tpr_dft<N, false>(v);
     }
     __syncthreads();
     if (active) {
@@ -473,7 +473,7 @@ __device__ __forceinline__ void c2r_b(const GenRowPass &p, const TprSmem &m, int
             const float2 A = sa[kk], B = sb[kk];
             v[k2] = up ? make_float2(A.x + B.y, B.x - A.y) : make_float2(A.x - B.y, A.y + B.x);
         }
-        tpr_dft<N, true>(v, m.tw, F1);
+        tpr_dft<N, true>(v);
         const float2 *t = m.Tt + k1;  // Tt[n2 F1 + k1], lanes along k1
 #pragma unroll
         for (int n2 = 1; n2 < N; ++n2) v[n2] = c_conj_mul(v[n2], t[n2 * F1]);
@@ -522,7 +522,7 @@ __device__ __forceinline__ void c2r_a(const GenRowPass &p, const TprSmem &m, int
     const float2 *src = m.S + n2 * (NL + 1) + l;
 #pragma unroll
     for (int k1 = 0; k1 < N; ++k1) v[k1] = src[k1 * GS];
-    tpr_dft<N, true>(v, m.tw, F2);
+    tpr_dft<N, true>(v);
     const RowRef ra = row_ref(p, r0 + l, p.r_s1, p.r_s2), rb = row_ref(p, r0 + NL + l, p.r_s1, p.r_s2);
     float *da = p.rdst + ra.off, *db = p.rdst + rb.off;
     float *ua = (p.fuse_update && p.dchem) ? p.dchem + ra.off : nullptr;
